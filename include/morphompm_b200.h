@@ -1,0 +1,162 @@
+/*
+ * morphompm_b200 -- C ABI of the B200 (sm_100a) MLS-MPM growth step.
+ *
+ * Plain C types only: device pointers, sizes, a cudaStream_t passed as void*.
+ * Every entry point returns an int status (MPM_OK == 0).  The library never
+ * allocates device memory: the caller sizes one workspace with
+ * mpm_plan_workspace_bytes() and one tape per recorded step with
+ * mpm_plan_tape_bytes(), and passes them in.  Device-side failures (non-finite
+ * state, particles that left the grid) are recorded in a status word that
+ * mpm_plan_read_status() returns.
+ *
+ * The reference implementation is the numpy package of 2nugu/morphompm; each
+ * entry point below names the reference function whose behaviour it replaces.
+ */
+#ifndef MORPHOMPM_B200_H
+#define MORPHOMPM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes (return values and bits of the device status word) ---- */
+#define MPM_OK               0
+#define MPM_ERR_ARG          1    /* bad argument (null pointer, bad size)            */
+#define MPM_ERR_CUDA         2    /* a CUDA runtime call failed                       */
+#define MPM_ERR_NONFINITE    4    /* NaN/Inf produced in state, stress or gradient    */
+#define MPM_WARN_OUTSIDE     8    /* a particle's stencil left the grid entirely     */
+#define MPM_ERR_TAPE        16    /* tape missing or recorded for another plan        */
+#define MPM_ERR_UNSUPPORTED 32    /* model kind / dtype not built                     */
+
+/* ---- constitutive model kinds (python/morphompm/constitutive.py) ---- */
+#define MPM_MODEL_NEOHOOKEAN        0   /* constitutive.py:25-39  */
+#define MPM_MODEL_HENCKY            1   /* constitutive.py:42-75  */
+#define MPM_MODEL_HERSCHEL_BULKLEY  2   /* constitutive.py:106-147 */
+
+/* ---- arithmetic types ---- */
+#define MPM_F32 4
+#define MPM_F64 8
+
+/* One scene of a batch: its grid, its material and its growth law.  A batch
+ * of one scene with growth_mode 0 is the reference's transfer.step on one
+ * SimConfig (python/morphompm/config.py:21-40). */
+typedef struct MpmScene {
+    int32_t shape[3];        /* nodes per axis (the reference has N,N,N)              */
+    int32_t model;           /* MPM_MODEL_*                                           */
+    int64_t p_begin, p_end;  /* this scene's particle range in the batch arrays       */
+    int32_t wall;            /* sticky nodes: index < wall or >= shape-wall (0 = none) */
+    int32_t clamp_lo[3];     /* sticky box [clamp_lo, clamp_hi) (empty if lo >= hi)    */
+    int32_t clamp_hi[3];
+    int32_t growth_mode;     /* 0: Fg read per particle; 1: Fg = g_p(t) I (see below) */
+    double dx, dt, damping, pmass, vol0;
+    double mass_eps;         /* grid nodes with mass <= mass_eps are inactive (1e-12)  */
+    double gravity[3];
+    double mu, lam;          /* neo-Hookean / Hencky Lame parameters                  */
+    double kappa, K, n_exp, tau_y, m_pap, eps; /* Herschel-Bulkley (constitutive.py:115) */
+    double growth_A;         /* growth_mode 1: g_p(t) = 1 + A*ramp(t)*phi_p            */
+    double ramp_steps;       /* ramp(t) = min(1,(t+1)/ramp_steps); 1 when <= 0          */
+} MpmScene;
+
+/* Particle arrays.  Element (p, c) of a 3-vector field lives at
+ * ptr[p*sp3 + c*sc3]; of a 3x3 field (row-major c = 3*i+j) at ptr[p*sp9 + c*sc9].
+ * (n,3)/(n,3,3) C-contiguous arrays use sp3=3,sc3=1,sp9=9,sc9=1.
+ * Fg may be NULL when every scene uses growth_mode 1. */
+typedef struct MpmParticles {
+    void *x, *v, *C, *F, *Fg;
+    int64_t sp3, sc3, sp9, sc9;
+} MpmParticles;
+
+/* Cotangents of a particle state.  Same layout rules as MpmParticles; the Fg
+ * cotangent is always double (it carries the growth-parameter gradient). */
+typedef struct MpmCotangents {
+    void *x, *v, *C, *F;
+    double *Fg;              /* may be NULL when every scene uses growth_mode 1 */
+    int64_t sp3, sc3, sp9, sc9;
+} MpmCotangents;
+
+/* Schedule knobs (picked by the autotuner; zeros select the defaults). */
+typedef struct MpmTuning {
+    int32_t tile_xy;             /* node tile edge in x and y: 4, 8 or 16 (z is fixed at 14) */
+    int32_t scatter_ctas_per_sm; /* persistent P2G grid = SMs x this (default 2)            */
+    int32_t scatter_oxb;         /* stencil x-offsets per pass: 3 (FP32 default) or 1       */
+    int32_t particle_block;      /* threads per block of the per-particle kernels (256)     */
+    int32_t active_tile_cap;     /* capacity of the active-tile list (0 = every tile)       */
+    float fp64_gap_thresh;       /* FP32 Hencky: relative singular-value gap below this is
+                                    recomputed in FP64 (0 selects 1e-4; <0 disables)        */
+} MpmTuning;
+
+typedef struct MpmPlan MpmPlan;   /* host-side plan (offsets, tile tables)         */
+
+/* Build a plan for a batch of scenes (host only, no CUDA calls).
+ * real_bytes is MPM_F32 or MPM_F64. */
+int mpm_plan_create(const MpmScene* scenes, int32_t n_scenes, int32_t real_bytes,
+                    const MpmTuning* tuning, MpmPlan** out);
+void mpm_plan_destroy(MpmPlan* plan);
+int mpm_plan_workspace_bytes(const MpmPlan* plan, size_t* bytes);
+int mpm_plan_tape_bytes(const MpmPlan* plan, size_t* bytes);
+int64_t mpm_plan_num_particles(const MpmPlan* plan);
+/* Upload the scene table and index tables into the workspace and clear the
+ * status word (stream-ordered; call once before the first step). */
+int mpm_plan_bind(MpmPlan* plan, void* workspace, void* stream);
+/* Copy the device status word into *status (synchronises the stream). */
+int mpm_plan_read_status(MpmPlan* plan, int32_t* status, void* stream);
+/* Number of FP32 Hencky evaluations that took the FP64 path since bind. */
+int mpm_plan_read_fp64_fallbacks(MpmPlan* plan, int64_t* count, void* stream);
+
+/* Optional per-particle growth field phi_p (growth_mode 1), real type. */
+int mpm_plan_set_growth_field(MpmPlan* plan, const void* phi);
+
+/* One forward MLS-MPM step for every scene of the batch:
+ * binning + cell sort, stress, P2G, grid update with boundary conditions,
+ * G2P with advection and the F update.
+ * Replaces python/morphompm/transfer.py:33-79 (step).
+ * `in` and `out` must not alias.  `tape` (mpm_plan_tape_bytes) may be NULL; if
+ * given it records what mpm_step_bwd needs for this step.  step_index is the t
+ * of the growth ramp. */
+int mpm_step_fwd(MpmPlan* plan, const MpmParticles* in, MpmParticles* out, int32_t advect,
+                 int32_t step_index, void* tape, void* stream);
+
+/* Reverse of mpm_step_fwd for the step recorded in `tape`.
+ * Replaces python/morphompm/transfer.py:82-158 (step_vjp).
+ * `in` is the step's input state, `out_C` the C of its output state.
+ * out_bar: cotangents of the output state; in_bar receives those of the input
+ * (Fg cotangent: in_bar->Fg = out_bar->Fg + local term; they may alias).
+ * growth_grad (per scene, double, may be NULL) is incremented by d loss / d A
+ * for scenes in growth_mode 1. */
+int mpm_step_bwd(MpmPlan* plan, const MpmParticles* in, const void* out_C,
+                 const MpmCotangents* out_bar, MpmCotangents* in_bar,
+                 double* growth_grad, int32_t advect, int32_t step_index,
+                 const void* tape, void* stream);
+
+/* Batched constitutive seam: tau = model.stress(F, Fg, C) for n particles of one
+ * scene's model.  Replaces constitutive.py:88-89,126-132. Arrays (n,3,3) C-contiguous. */
+int mpm_stress(const MpmScene* scene, int32_t real_bytes, int64_t n, const void* F,
+               const void* Fg, const void* C, void* tau, void* stream);
+/* (F_bar, Fg_bar, C_bar) = model.stress_vjp(F, Fg, C, tau_bar).
+ * Replaces constitutive.py:91-93,134-147. */
+int mpm_stress_vjp(const MpmScene* scene, int32_t real_bytes, int64_t n, const void* F,
+                   const void* Fg, const void* C, const void* tau_bar, void* F_bar,
+                   void* Fg_bar, void* C_bar, void* stream);
+
+/* Cell keys of the binning step (the stencil base of transfer.py:18-21, shifted
+ * by +2 per axis and flattened over the (shape+2)^3 padded cells, z fastest;
+ * particles whose stencil misses the grid get (shape+2)^3).  x is (n,3). */
+int mpm_bin_keys(const MpmScene* scene, int32_t real_bytes, int64_t n, const void* x,
+                 int32_t* keys, void* stream);
+
+/* Loss seeds and values (python/morphompm/integrate.py:41-52). Per scene,
+ * double loss[s]; F_bar / x_bar are written (not accumulated). */
+int mpm_loss_detF(MpmPlan* plan, const void* F, int64_t sp9, int64_t sc9, double* loss,
+                  void* F_bar, void* stream);
+int mpm_loss_mse(MpmPlan* plan, const void* x, int64_t sp3, int64_t sc3, const void* x_obs,
+                 double* loss, void* x_bar, void* stream);
+
+int mpm_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MORPHOMPM_B200_H */

@@ -1,0 +1,118 @@
+"""[2] Constitutive seam -- the reference's pluggable models
+(python/morphompm/constitutive.py:1-147) with the same interface:
+
+    model.stress(F, Fg, C=None)           -> tau   (Kirchhoff, 3x3 sym)
+    model.stress_vjp(F, Fg, C, tau_bar)   -> (F_bar, Fg_bar, C_bar)
+
+Both run on the GPU (``mpm_stress`` / ``mpm_stress_vjp``) for a single 3x3
+matrix or a batch (n,3,3).  numpy inputs come back as numpy, torch CUDA inputs
+stay on the device.  Inside ``transfer.step`` the same device code is fused into
+the P2G prepass and the reverse particle kernel; these objects carry the model
+kind and parameters that the step kernels read.
+"""
+from __future__ import annotations
+
+import ctypes as ct
+
+import numpy as np
+
+from . import _lib as L
+from .config import Material
+from .devarray import to_device, like_input
+
+
+class _Model:
+    kind = None
+
+    def scene_fields(self) -> dict:
+        raise NotImplementedError
+
+    def _scene(self):
+        from .runtime import SceneSpec
+        f = self.scene_fields()
+        return SceneSpec(shape=(1, 1, 1), n=0, dx=1.0, dt=0.0, damping=0.0, pmass=0.0, vol0=0.0, **f).to_c(0)
+
+    def stress(self, F, Fg, C=None):
+        lib = L.load()
+        (Fd, Fgd, Cd), ref, single = _prep([F, Fg, C])
+        import torch
+        tau = torch.empty_like(Fd)
+        from .runtime import dtype_bytes, stream_ptr
+        L.check(lib.mpm_stress(ct.byref(self._scene()), dtype_bytes(Fd.dtype), Fd.shape[0], Fd.data_ptr(),
+                               Fgd.data_ptr(), Cd.data_ptr() if Cd is not None else None, tau.data_ptr(),
+                               ct.c_void_p(stream_ptr())), "mpm_stress")
+        return like_input(tau[0] if single else tau, ref)
+
+    def stress_vjp(self, F, Fg, C, tau_bar):
+        lib = L.load()
+        (Fd, Fgd, Cd, tb), ref, single = _prep([F, Fg, C, tau_bar])
+        import torch
+        Fb, Fgb, Cb = torch.empty_like(Fd), torch.empty_like(Fd), torch.empty_like(Fd)
+        from .runtime import dtype_bytes, stream_ptr
+        L.check(lib.mpm_stress_vjp(ct.byref(self._scene()), dtype_bytes(Fd.dtype), Fd.shape[0], Fd.data_ptr(),
+                                   Fgd.data_ptr(), Cd.data_ptr() if Cd is not None else None, tb.data_ptr(),
+                                   Fb.data_ptr(), Fgb.data_ptr(), Cb.data_ptr(), ct.c_void_p(stream_ptr())),
+                "mpm_stress_vjp")
+        out = (Fb, Fgb, Cb)
+        if single:
+            out = tuple(o[0] for o in out)
+        return tuple(like_input(o, ref) for o in out)
+
+
+def _prep(arrs):
+    """Move a list of (3,3)/(n,3,3) arrays (None allowed) to contiguous device tensors."""
+    ref = next(a for a in arrs if a is not None)
+    single = (ref.ndim == 2)
+    dev = to_device(ref)
+    out = []
+    for a in arrs:
+        if a is None:
+            out.append(None)
+            continue
+        t = to_device(a, dtype=dev.dtype, device=dev.device)
+        if single:
+            t = t.reshape(1, 3, 3)
+        out.append(t.contiguous())
+    return out, ref, single
+
+
+class _ElasticModel(_Model):
+    """Rate-independent: C ignored, C_bar = 0 (constitutive.py:79-93)."""
+
+    def __init__(self, material: Material):
+        self.mu = material.mu
+        self.lam = material.lam
+
+    def scene_fields(self):
+        return dict(model=self.kind, mu=self.mu, lam=self.lam)
+
+
+class NeoHookean(_ElasticModel):
+    """tau = mu (Fe Fe^T - I) + lam ln J I   (constitutive.py:25-39)."""
+    kind = L.MODEL_NEOHOOKEAN
+
+
+class Hencky(_ElasticModel):
+    """tau = U diag(2 mu ln s + lam sum ln s) U^T  (constitutive.py:42-75)."""
+    kind = L.MODEL_HENCKY
+
+
+class HerschelBulkley(_Model):
+    """Rate-dependent bioink, Papanastasiou-regularised (constitutive.py:106-147)."""
+    kind = L.MODEL_HERSCHEL_BULKLEY
+
+    def __init__(self, kappa=1.0e4, K=1.0, n=0.5, tau_y=50.0, m=100.0, eps=1e-4):
+        self.kappa, self.K, self.n, self.tau_y, self.m, self.eps = kappa, K, n, tau_y, m, eps
+
+    def scene_fields(self):
+        return dict(model=self.kind, hb=dict(kappa=self.kappa, K=self.K, n=self.n, tau_y=self.tau_y,
+                                             m=self.m, eps=self.eps))
+
+
+def model_fields(model) -> dict:
+    """Scene fields of a built-in model; anything else is rejected (the GPU
+    path has no CPU fallback for a Python-defined material)."""
+    if isinstance(model, _Model):
+        return model.scene_fields()
+    raise TypeError(f"{type(model).__name__} is not a built-in morphompm_b200 model "
+                    "(NeoHookean, Hencky, HerschelBulkley)")

@@ -1,0 +1,509 @@
+// Host side of the C ABI (include/morphompm_b200.h): plan construction,
+// workspace/tape layout, and the launch sequences of one forward and one
+// reverse growth step.  No device memory is allocated here.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "../../include/morphompm_b200.h"
+#include "mpm_common.cuh"
+#include "constitutive.cuh"
+#include "sort.cuh"
+#include "mpm_kernels.cuh"
+
+using namespace mpm;
+
+namespace {
+
+constexpr size_t ALIGN = 256;
+inline size_t align_up(size_t v) { return (v + ALIGN - 1) / ALIGN * ALIGN; }
+
+struct Layout {
+    size_t off = 0;
+    size_t take(size_t bytes) {
+        size_t o = off;
+        off = align_up(off + bytes);
+        return o;
+    }
+};
+
+}  // namespace
+
+struct MpmPlan {
+    std::vector<MpmScene> scenes;
+    std::vector<SceneAux> aux;
+    std::vector<int> scene_of;
+    std::vector<int> tile_scene;
+    int real_bytes = 8;
+    MpmTuning tune{};
+    long long n = 0, n_tiles = 0, n_keys = 0;
+    int key_bits = 1, passes = 1, nblk_sort = 1;
+    int TN = 0, active_cap = 0;
+    bool any_growth = false;
+    // workspace offsets
+    size_t o_scenes, o_aux, o_scene_of, o_tile_scene, o_status, o_cell_first, o_cell_last, o_tile_flag;
+    size_t o_keys, o_kalt0, o_valt0, o_kalt1, o_valt1, o_hist, o_totals, o_payload, o_gridb, o_dbuf, o_tape;
+    size_t ws_bytes = 0;
+    // tape offsets
+    size_t t_skeys, t_perm, t_slot, t_active, t_nact, t_grid, tape_bytes = 0;
+    char* ws = nullptr;
+    const void* phi = nullptr;
+    int n_sm = 148;
+};
+
+namespace {
+
+template <typename T>
+T* at(MpmPlan* P, size_t off) { return reinterpret_cast<T*>(P->ws + off); }
+
+Ctx make_ctx(MpmPlan* P) {
+    Ctx c;
+    c.scenes = at<const MpmScene>(P, P->o_scenes);
+    c.aux = at<const SceneAux>(P, P->o_aux);
+    c.scene_of = at<const int>(P, P->o_scene_of);
+    c.tile_scene = at<const int>(P, P->o_tile_scene);
+    c.status = at<int>(P, P->o_status);
+    c.fallbacks = reinterpret_cast<unsigned long long*>(P->ws + P->o_status + 64);
+    c.cell_first = at<int>(P, P->o_cell_first);
+    c.cell_last = at<int>(P, P->o_cell_last);
+    c.tile_flag = at<int>(P, P->o_tile_flag);
+    c.phi = P->phi;
+    c.n = P->n;
+    c.n_tiles = P->n_tiles;
+    c.n_scenes = (int)P->scenes.size();
+    c.tile_xy = P->tune.tile_xy;
+    c.active_cap = P->active_cap;
+    c.gap_thresh = P->tune.fp64_gap_thresh < 0 ? 0.0f : P->tune.fp64_gap_thresh;
+    return c;
+}
+
+template <typename R>
+Tape<R> make_tape(MpmPlan* P, char* t) {
+    Tape<R> tp;
+    tp.skeys = reinterpret_cast<unsigned*>(t + P->t_skeys);
+    tp.perm = reinterpret_cast<unsigned*>(t + P->t_perm);
+    tp.tile_slot = reinterpret_cast<int*>(t + P->t_slot);
+    tp.active = reinterpret_cast<int*>(t + P->t_active);
+    tp.n_active = reinterpret_cast<int*>(t + P->t_nact);
+    tp.grid = reinterpret_cast<R*>(t + P->t_grid);
+    return tp;
+}
+
+inline int grid_for(long long n, int block) { return (int)std::max<long long>(1, (n + block - 1) / block); }
+
+inline int check_launch() {
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? MPM_OK : MPM_ERR_CUDA;
+}
+
+template <typename R, int T, int MODE>
+void* scatter_fn(int oxb) {
+    if constexpr (sizeof(R) == 4) {
+        if (oxb == 3) return (void*)scatter_kernel<R, T, MODE, 3>;
+    }
+    return (void*)scatter_kernel<R, T, MODE, 1>;
+}
+
+template <typename R, int MODE>
+void* scatter_dispatch(int T, int oxb) {
+    if (T == 4) return scatter_fn<R, 4, MODE>(oxb);
+    if (T == 16) return scatter_fn<R, 16, MODE>(oxb);
+    return scatter_fn<R, 8, MODE>(oxb);
+}
+
+template <typename R>
+size_t scatter_smem(int T, int mode) { return (size_t)T * T * TILE_Z * (mode == 0 ? 4 : 3) * sizeof(R); }
+
+template <typename R>
+int launch_scatter(MpmPlan* P, int mode, const Ctx& ctx, const R* payload, const int* active, const int* nact,
+                   R* grid_out, const R* grid_fwd, int advect, cudaStream_t st) {
+    const int T = P->tune.tile_xy;
+    int oxb = P->tune.scatter_oxb;
+    void* fn = mode == 0 ? scatter_dispatch<R, 0>(T, oxb) : scatter_dispatch<R, 1>(T, oxb);
+    size_t smem = scatter_smem<R>(T, mode);
+    int ctas = P->n_sm * std::max(1, P->tune.scatter_ctas_per_sm);
+    ctas = std::max(1, std::min(ctas, P->active_cap));
+    void* args[] = {(void*)&ctx, (void*)&payload, (void*)&active, (void*)&nact, (void*)&grid_out,
+                    (void*)&grid_fwd, (void*)&advect};
+    cudaError_t e = cudaLaunchKernel(fn, dim3(ctas), dim3(256), args, smem, st);
+    return e == cudaSuccess ? MPM_OK : MPM_ERR_CUDA;
+}
+
+template <typename R>
+int set_smem_attrs(MpmPlan* P) {
+    const int T = P->tune.tile_xy;
+    for (int mode = 0; mode < 2; ++mode) {
+        for (int oxb : {1, 3}) {
+            void* fn = mode == 0 ? scatter_dispatch<R, 0>(T, oxb) : scatter_dispatch<R, 1>(T, oxb);
+            size_t smem = scatter_smem<R>(T, mode);
+            if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+                return MPM_ERR_CUDA;
+        }
+    }
+    return MPM_OK;
+}
+
+// stable LSD radix sort of the binning keys -> tape (skeys, perm)
+int run_sort(MpmPlan* P, const unsigned* keys, unsigned* skeys, unsigned* perm, cudaStream_t st) {
+    unsigned* kalt[2] = {at<unsigned>(P, P->o_kalt0), at<unsigned>(P, P->o_kalt1)};
+    unsigned* valt[2] = {at<unsigned>(P, P->o_valt0), at<unsigned>(P, P->o_valt1)};
+    unsigned* hist = at<unsigned>(P, P->o_hist);
+    unsigned* totals = at<unsigned>(P, P->o_totals);
+    const int nblk = P->nblk_sort;
+    const unsigned* ksrc = keys;
+    const unsigned* vsrc = nullptr;
+    for (int pass = 0; pass < P->passes; ++pass) {
+        const int shift = pass * RADIX_BITS;
+        unsigned* kdst = (pass == P->passes - 1) ? skeys : kalt[pass & 1];
+        unsigned* vdst = (pass == P->passes - 1) ? perm : valt[pass & 1];
+        radix_hist_kernel<<<nblk, SORT_THREADS, 0, st>>>(ksrc, P->n, shift, hist, nblk);
+        radix_rowsum_kernel<<<RADIX, 256, 0, st>>>(hist, nblk, totals);
+        radix_rowscan_kernel<<<RADIX, 256, 0, st>>>(hist, nblk, totals);
+        radix_scatter_kernel<<<nblk, SORT_THREADS, 0, st>>>(ksrc, vsrc, P->n, shift, hist, nblk, kdst, vdst);
+        ksrc = kdst;
+        vsrc = vdst;
+    }
+    return check_launch();
+}
+
+template <typename R, int T>
+int step_fwd_T(MpmPlan* P, const MpmParticles& in, MpmParticles& out, int advect, int t, char* tape,
+               cudaStream_t st) {
+    Ctx ctx = make_ctx(P);
+    Tape<R> tp = make_tape<R>(P, tape);
+    const int B = P->tune.particle_block;
+    const int g = grid_for(P->n, B);
+    unsigned* keys = at<unsigned>(P, P->o_keys);
+    R* payload = at<R>(P, P->o_payload);
+    bin_kernel<R><<<g, B, 0, st>>>(ctx, in, keys);
+    int rc = run_sort(P, keys, tp.skeys, tp.perm, st);
+    if (rc) return rc;
+    mark_kernel<<<g, B, 0, st>>>(ctx, tp.skeys, 1);
+    compact_tiles_kernel<<<1, 1024, 0, st>>>(ctx.tile_flag, P->n_tiles, tp.tile_slot, tp.active, tp.n_active,
+                                             P->active_cap, ctx.status);
+    prepass_kernel<R><<<g, B, 0, st>>>(ctx, in, tp.perm, payload, t);
+    rc = check_launch();
+    if (rc) return rc;
+    rc = launch_scatter<R>(P, 0, ctx, payload, tp.active, tp.n_active, tp.grid, nullptr, advect, st);
+    if (rc) return rc;
+    g2p_kernel<R, T><<<g, B, 0, st>>>(ctx, tp, in, out, advect);
+    return check_launch();
+}
+
+template <typename R, int T>
+int step_bwd_T(MpmPlan* P, const MpmParticles& in, const void* outC, const MpmCotangents& ob, MpmCotangents& ib,
+               double* growth_grad, int advect, int t, const char* tape, cudaStream_t st) {
+    Ctx ctx = make_ctx(P);
+    Tape<R> tp = make_tape<R>(P, const_cast<char*>(tape));
+    const int B = P->tune.particle_block;
+    const int g = grid_for(P->n, B);
+    R* payload = at<R>(P, P->o_payload);
+    R* gridb = at<R>(P, P->o_gridb);
+    double* dbuf = at<double>(P, P->o_dbuf);
+    mark_kernel<<<g, B, 0, st>>>(ctx, tp.skeys, 0);
+    bwd_payload_kernel<R><<<g, B, 0, st>>>(ctx, tp.perm, in, ob, payload, advect);
+    int rc = check_launch();
+    if (rc) return rc;
+    rc = launch_scatter<R>(P, 1, ctx, payload, tp.active, tp.n_active, gridb, tp.grid, advect, st);
+    if (rc) return rc;
+    bool want_dA = growth_grad != nullptr && P->any_growth;
+    bwd_particle_kernel<R, T><<<g, B, 0, st>>>(ctx, tp, gridb, in, static_cast<const R*>(outC), ob, ib,
+                                               want_dA ? dbuf : nullptr, advect, t);
+    if (want_dA)
+        scene_reduce_kernel<<<(int)P->scenes.size(), 256, 0, st>>>(ctx, dbuf, growth_grad, 1, 0);
+    return check_launch();
+}
+
+template <typename R>
+int step_fwd_R(MpmPlan* P, const MpmParticles& in, MpmParticles& out, int advect, int t, char* tape,
+               cudaStream_t st) {
+    switch (P->tune.tile_xy) {
+        case 4: return step_fwd_T<R, 4>(P, in, out, advect, t, tape, st);
+        case 16: return step_fwd_T<R, 16>(P, in, out, advect, t, tape, st);
+        default: return step_fwd_T<R, 8>(P, in, out, advect, t, tape, st);
+    }
+}
+template <typename R>
+int step_bwd_R(MpmPlan* P, const MpmParticles& in, const void* outC, const MpmCotangents& ob, MpmCotangents& ib,
+               double* gg, int advect, int t, const char* tape, cudaStream_t st) {
+    switch (P->tune.tile_xy) {
+        case 4: return step_bwd_T<R, 4>(P, in, outC, ob, ib, gg, advect, t, tape, st);
+        case 16: return step_bwd_T<R, 16>(P, in, outC, ob, ib, gg, advect, t, tape, st);
+        default: return step_bwd_T<R, 8>(P, in, outC, ob, ib, gg, advect, t, tape, st);
+    }
+}
+
+bool scene_ok(const MpmScene& s) {
+    for (int d = 0; d < 3; ++d)
+        if (s.shape[d] < 1 || s.shape[d] > 4096) return false;
+    if (s.model < 0 || s.model > 2) return false;
+    if (!(s.dx > 0) || !(s.dt >= 0)) return false;
+    if (s.p_end < s.p_begin) return false;
+    return true;
+}
+
+}  // namespace
+
+extern "C" {
+
+int mpm_version(void) { return 1; }
+
+int mpm_plan_create(const MpmScene* scenes, int32_t n_scenes, int32_t real_bytes, const MpmTuning* tuning,
+                    MpmPlan** out) {
+    if (!scenes || n_scenes < 1 || !out || (real_bytes != 4 && real_bytes != 8)) return MPM_ERR_ARG;
+    MpmPlan* P = new (std::nothrow) MpmPlan();
+    if (!P) return MPM_ERR_ARG;
+    P->real_bytes = real_bytes;
+    if (tuning) P->tune = *tuning;
+    if (P->tune.tile_xy != 4 && P->tune.tile_xy != 16) P->tune.tile_xy = 8;
+    if (P->tune.scatter_ctas_per_sm <= 0) P->tune.scatter_ctas_per_sm = 2;
+    if (P->tune.scatter_oxb != 1 && P->tune.scatter_oxb != 3) P->tune.scatter_oxb = real_bytes == 4 ? 3 : 1;
+    if (real_bytes == 8) P->tune.scatter_oxb = 1;
+    if (P->tune.particle_block <= 0 || P->tune.particle_block > 1024 || P->tune.particle_block % 32)
+        P->tune.particle_block = 256;
+    if (P->tune.fp64_gap_thresh == 0.0f) P->tune.fp64_gap_thresh = 1e-4f;
+    const int T = P->tune.tile_xy;
+    P->TN = T * T * TILE_Z;
+    long long cell = 0, tile = 0, pcur = 0;
+    for (int s = 0; s < n_scenes; ++s) {
+        const MpmScene& sc = scenes[s];
+        if (!scene_ok(sc) || sc.p_begin != pcur) { delete P; return MPM_ERR_ARG; }
+        pcur = sc.p_end;
+        SceneAux a;
+        a.cell_begin = cell;
+        a.ncells = (sc.shape[0] + 2) * (sc.shape[1] + 2) * (sc.shape[2] + 2);
+        a.ntile[0] = (sc.shape[0] + T - 1) / T;
+        a.ntile[1] = (sc.shape[1] + T - 1) / T;
+        a.ntile[2] = (sc.shape[2] + TILE_Z - 1) / TILE_Z;
+        a.tile_begin = tile;
+        cell += (long long)a.ncells + 1;
+        tile += (long long)a.ntile[0] * a.ntile[1] * a.ntile[2];
+        P->scenes.push_back(sc);
+        P->aux.push_back(a);
+        if (sc.growth_mode == 1) P->any_growth = true;
+        for (long long p = sc.p_begin; p < sc.p_end; ++p) P->scene_of.push_back(s);
+        for (long long k = a.tile_begin; k < tile; ++k) P->tile_scene.push_back(s);
+    }
+    if (cell >= (1LL << 31) || pcur >= (1LL << 31) || pcur < 1) { delete P; return MPM_ERR_ARG; }
+    P->n = pcur;
+    P->n_tiles = tile;
+    P->n_keys = cell;
+    int bits = 1;
+    while ((1LL << bits) < cell) ++bits;
+    P->key_bits = bits;
+    P->passes = (bits + RADIX_BITS - 1) / RADIX_BITS;
+    P->nblk_sort = (int)((P->n + SORT_TILE - 1) / SORT_TILE);
+    P->active_cap = (int)P->n_tiles;
+    if (P->tune.active_tile_cap > 0 && P->tune.active_tile_cap < P->active_cap) P->active_cap = P->tune.active_tile_cap;
+
+    const size_t R = (size_t)real_bytes, n = (size_t)P->n, nt = (size_t)P->n_tiles;
+    Layout tl;
+    P->t_skeys = tl.take(n * 4);
+    P->t_perm = tl.take(n * 4);
+    P->t_slot = tl.take(nt * 4);
+    P->t_active = tl.take((size_t)P->active_cap * 4);
+    P->t_nact = tl.take(4);
+    P->t_grid = tl.take((size_t)P->active_cap * P->TN * 4 * R);
+    P->tape_bytes = tl.off;
+
+    Layout L;
+    P->o_scenes = L.take(sizeof(MpmScene) * P->scenes.size());
+    P->o_aux = L.take(sizeof(SceneAux) * P->aux.size());
+    P->o_scene_of = L.take(n * 4);
+    P->o_tile_scene = L.take(nt * 4);
+    P->o_status = L.take(128);
+    P->o_cell_first = L.take((size_t)P->n_keys * 4);
+    P->o_cell_last = L.take((size_t)P->n_keys * 4);
+    P->o_tile_flag = L.take(nt * 4);
+    P->o_keys = L.take(n * 4);
+    P->o_kalt0 = L.take(n * 4);
+    P->o_valt0 = L.take(n * 4);
+    P->o_kalt1 = L.take(n * 4);
+    P->o_valt1 = L.take(n * 4);
+    P->o_hist = L.take((size_t)RADIX * P->nblk_sort * 4);
+    P->o_totals = L.take(RADIX * 4);
+    P->o_payload = L.take(n * PAYLOAD * R);
+    P->o_gridb = L.take((size_t)P->active_cap * P->TN * 4 * R);
+    P->o_dbuf = L.take(n * 8);
+    P->o_tape = L.take(P->tape_bytes);
+    P->ws_bytes = L.off;
+    *out = P;
+    return MPM_OK;
+}
+
+void mpm_plan_destroy(MpmPlan* plan) { delete plan; }
+
+int mpm_plan_workspace_bytes(const MpmPlan* P, size_t* bytes) {
+    if (!P || !bytes) return MPM_ERR_ARG;
+    *bytes = P->ws_bytes;
+    return MPM_OK;
+}
+int mpm_plan_tape_bytes(const MpmPlan* P, size_t* bytes) {
+    if (!P || !bytes) return MPM_ERR_ARG;
+    *bytes = P->tape_bytes;
+    return MPM_OK;
+}
+int64_t mpm_plan_num_particles(const MpmPlan* P) { return P ? P->n : -1; }
+
+int mpm_plan_bind(MpmPlan* P, void* workspace, void* stream) {
+    if (!P || !workspace || (reinterpret_cast<uintptr_t>(workspace) % ALIGN) != 0) return MPM_ERR_ARG;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    P->ws = static_cast<char*>(workspace);
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return MPM_ERR_CUDA;
+    cudaDeviceGetAttribute(&P->n_sm, cudaDevAttrMultiProcessorCount, dev);
+    int rc = P->real_bytes == 4 ? set_smem_attrs<float>(P) : set_smem_attrs<double>(P);
+    if (rc) return rc;
+    if (cudaMemcpyAsync(P->ws + P->o_scenes, P->scenes.data(), sizeof(MpmScene) * P->scenes.size(),
+                        cudaMemcpyHostToDevice, st) != cudaSuccess ||
+        cudaMemcpyAsync(P->ws + P->o_aux, P->aux.data(), sizeof(SceneAux) * P->aux.size(),
+                        cudaMemcpyHostToDevice, st) != cudaSuccess ||
+        cudaMemcpyAsync(P->ws + P->o_scene_of, P->scene_of.data(), 4 * P->scene_of.size(),
+                        cudaMemcpyHostToDevice, st) != cudaSuccess ||
+        cudaMemcpyAsync(P->ws + P->o_tile_scene, P->tile_scene.data(), 4 * P->tile_scene.size(),
+                        cudaMemcpyHostToDevice, st) != cudaSuccess ||
+        cudaMemsetAsync(P->ws + P->o_status, 0, 128, st) != cudaSuccess ||
+        cudaMemsetAsync(P->ws + P->o_cell_first, 0, (size_t)P->n_keys * 4, st) != cudaSuccess ||
+        cudaMemsetAsync(P->ws + P->o_cell_last, 0, (size_t)P->n_keys * 4, st) != cudaSuccess ||
+        cudaMemsetAsync(P->ws + P->o_tile_flag, 0, (size_t)P->n_tiles * 4, st) != cudaSuccess)
+        return MPM_ERR_CUDA;
+    // the host tables are read by the copies above: wait before returning
+    if (cudaStreamSynchronize(st) != cudaSuccess) return MPM_ERR_CUDA;
+    return MPM_OK;
+}
+
+int mpm_plan_read_status(MpmPlan* P, int32_t* status, void* stream) {
+    if (!P || !P->ws || !status) return MPM_ERR_ARG;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (cudaMemcpyAsync(status, P->ws + P->o_status, 4, cudaMemcpyDeviceToHost, st) != cudaSuccess) return MPM_ERR_CUDA;
+    return cudaStreamSynchronize(st) == cudaSuccess ? MPM_OK : MPM_ERR_CUDA;
+}
+
+int mpm_plan_read_fp64_fallbacks(MpmPlan* P, int64_t* count, void* stream) {
+    if (!P || !P->ws || !count) return MPM_ERR_ARG;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (cudaMemcpyAsync(count, P->ws + P->o_status + 64, 8, cudaMemcpyDeviceToHost, st) != cudaSuccess)
+        return MPM_ERR_CUDA;
+    return cudaStreamSynchronize(st) == cudaSuccess ? MPM_OK : MPM_ERR_CUDA;
+}
+
+int mpm_plan_set_growth_field(MpmPlan* P, const void* phi) {
+    if (!P) return MPM_ERR_ARG;
+    P->phi = phi;
+    return MPM_OK;
+}
+
+int mpm_step_fwd(MpmPlan* P, const MpmParticles* in, MpmParticles* out, int32_t advect, int32_t step_index,
+                 void* tape, void* stream) {
+    if (!P || !P->ws || !in || !out || !in->x || !in->v || !in->C || !in->F || !out->x || !out->v || !out->C ||
+        !out->F || in->x == out->x || in->F == out->F)
+        return MPM_ERR_ARG;
+    for (const MpmScene& s : P->scenes)
+        if (s.growth_mode == 0 && !in->Fg) return MPM_ERR_ARG;
+    char* tp = tape ? static_cast<char*>(tape) : P->ws + P->o_tape;
+    if (reinterpret_cast<uintptr_t>(tp) % ALIGN) return MPM_ERR_ARG;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    return P->real_bytes == 4 ? step_fwd_R<float>(P, *in, *out, advect, step_index, tp, st)
+                              : step_fwd_R<double>(P, *in, *out, advect, step_index, tp, st);
+}
+
+int mpm_step_bwd(MpmPlan* P, const MpmParticles* in, const void* out_C, const MpmCotangents* out_bar,
+                 MpmCotangents* in_bar, double* growth_grad, int32_t advect, int32_t step_index, const void* tape,
+                 void* stream) {
+    if (!P || !P->ws || !in || !out_C || !out_bar || !in_bar || !tape) return MPM_ERR_ARG;
+    if (!out_bar->x || !out_bar->v || !out_bar->C || !out_bar->F || !in_bar->x || !in_bar->v || !in_bar->C ||
+        !in_bar->F)
+        return MPM_ERR_ARG;
+    if (in_bar->x == out_bar->x || in_bar->v == out_bar->v || in_bar->C == out_bar->C || in_bar->F == out_bar->F)
+        return MPM_ERR_ARG;
+    for (const MpmScene& s : P->scenes)
+        if (s.growth_mode == 0 && !in->Fg) return MPM_ERR_ARG;
+    if (reinterpret_cast<uintptr_t>(tape) % ALIGN) return MPM_ERR_ARG;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    return P->real_bytes == 4
+               ? step_bwd_R<float>(P, *in, out_C, *out_bar, *in_bar, growth_grad, advect, step_index,
+                                   static_cast<const char*>(tape), st)
+               : step_bwd_R<double>(P, *in, out_C, *out_bar, *in_bar, growth_grad, advect, step_index,
+                                    static_cast<const char*>(tape), st);
+}
+
+int mpm_stress(const MpmScene* scene, int32_t real_bytes, int64_t n, const void* F, const void* Fg, const void* C,
+               void* tau, void* stream) {
+    if (!scene || n < 0 || !F || !Fg || !tau || (real_bytes != 4 && real_bytes != 8)) return MPM_ERR_ARG;
+    if (n == 0) return MPM_OK;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    int g = grid_for(n, 256);
+    if (real_bytes == 4)
+        stress_kernel<float><<<g, 256, 0, st>>>(*scene, n, (const float*)F, (const float*)Fg, (const float*)C,
+                                                (float*)tau, 1e-4f);
+    else
+        stress_kernel<double><<<g, 256, 0, st>>>(*scene, n, (const double*)F, (const double*)Fg,
+                                                 (const double*)C, (double*)tau, 0.0f);
+    return check_launch();
+}
+
+int mpm_stress_vjp(const MpmScene* scene, int32_t real_bytes, int64_t n, const void* F, const void* Fg,
+                   const void* C, const void* tau_bar, void* F_bar, void* Fg_bar, void* C_bar, void* stream) {
+    if (!scene || n < 0 || !F || !Fg || !tau_bar || !F_bar || !Fg_bar || (real_bytes != 4 && real_bytes != 8))
+        return MPM_ERR_ARG;
+    if (n == 0) return MPM_OK;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    int g = grid_for(n, 256);
+    if (real_bytes == 4)
+        stress_vjp_kernel<float><<<g, 256, 0, st>>>(*scene, n, (const float*)F, (const float*)Fg, (const float*)C,
+                                                    (const float*)tau_bar, (float*)F_bar, (float*)Fg_bar,
+                                                    (float*)C_bar, 1e-4f);
+    else
+        stress_vjp_kernel<double><<<g, 256, 0, st>>>(*scene, n, (const double*)F, (const double*)Fg,
+                                                     (const double*)C, (const double*)tau_bar, (double*)F_bar,
+                                                     (double*)Fg_bar, (double*)C_bar, 0.0f);
+    return check_launch();
+}
+
+int mpm_bin_keys(const MpmScene* scene, int32_t real_bytes, int64_t n, const void* x, int32_t* keys, void* stream) {
+    if (!scene || n < 0 || !x || !keys || (real_bytes != 4 && real_bytes != 8)) return MPM_ERR_ARG;
+    if (n == 0) return MPM_OK;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    int g = grid_for(n, 256);
+    if (real_bytes == 4)
+        bin_keys_single<float><<<g, 256, 0, st>>>(*scene, n, (const float*)x, keys);
+    else
+        bin_keys_single<double><<<g, 256, 0, st>>>(*scene, n, (const double*)x, keys);
+    return check_launch();
+}
+
+int mpm_loss_detF(MpmPlan* P, const void* F, int64_t sp9, int64_t sc9, double* loss, void* F_bar, void* stream) {
+    if (!P || !P->ws || !F || !loss) return MPM_ERR_ARG;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    Ctx ctx = make_ctx(P);
+    double* dbuf = at<double>(P, P->o_dbuf);
+    int g = grid_for(P->n, 256);
+    if (P->real_bytes == 4)
+        loss_detF_kernel<float><<<g, 256, 0, st>>>(ctx, (const float*)F, sp9, sc9, dbuf, (float*)F_bar);
+    else
+        loss_detF_kernel<double><<<g, 256, 0, st>>>(ctx, (const double*)F, sp9, sc9, dbuf, (double*)F_bar);
+    scene_reduce_kernel<<<(int)P->scenes.size(), 256, 0, st>>>(ctx, dbuf, loss, 0, 0);
+    return check_launch();
+}
+
+int mpm_loss_mse(MpmPlan* P, const void* x, int64_t sp3, int64_t sc3, const void* x_obs, double* loss, void* x_bar,
+                 void* stream) {
+    if (!P || !P->ws || !x || !x_obs || !loss) return MPM_ERR_ARG;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    Ctx ctx = make_ctx(P);
+    double* dbuf = at<double>(P, P->o_dbuf);
+    int g = grid_for(P->n, 256);
+    if (P->real_bytes == 4)
+        loss_mse_kernel<float><<<g, 256, 0, st>>>(ctx, (const float*)x, sp3, sc3, (const float*)x_obs, dbuf,
+                                                  (float*)x_bar);
+    else
+        loss_mse_kernel<double><<<g, 256, 0, st>>>(ctx, (const double*)x, sp3, sc3, (const double*)x_obs, dbuf,
+                                                   (double*)x_bar);
+    scene_reduce_kernel<<<(int)P->scenes.size(), 256, 0, st>>>(ctx, dbuf, loss, 0, 1);
+    return check_launch();
+}
+
+}  // extern "C"

@@ -1,0 +1,372 @@
+// Constitutive models of the growth step, forward Kirchhoff stress and the
+// hand-written vector-Jacobian products, on register-resident 3x3 matrices.
+//
+//   neo-Hookean        python/morphompm/constitutive.py:25-39
+//   Hencky             python/morphompm/constitutive.py:42-75
+//   Herschel-Bulkley   python/morphompm/constitutive.py:106-147
+//
+// Morphoelastic kinematics Fe = F Fg^{-1}.  Hencky is evaluated as an
+// isotropic function of b = Fe Fe^T through a symmetric 3x3 eigensolve
+// (cyclic Jacobi rotations, Rutishauser's update), which is equivalent to the
+// reference's SVD form tau = U diag(2 mu ln s + lam sum ln s) U^T since b = U S^2 U^T.
+#pragma once
+
+#include "mpm_common.cuh"
+
+namespace mpm {
+
+// ---------------------------------------------------------------------------
+// symmetric 3x3 eigen-decomposition by cyclic Jacobi rotations.
+// On return lam[i] are the eigenvalues and column i of V (row-major) the
+// corresponding unit eigenvector.
+// ---------------------------------------------------------------------------
+template <typename R>
+__device__ __forceinline__ void jacobi_rotate(R A[3][3], R V[9], int p, int q) {
+    R apq = A[p][q];
+    if (apq == R(0)) return;
+    R theta = (A[q][q] - A[p][p]) / (R(2) * apq);
+    R t = R(1) / (d_abs(theta) + d_sqrt(theta * theta + R(1)));
+    if (theta < R(0)) t = -t;
+    R c = R(1) / d_sqrt(t * t + R(1));
+    R s = t * c;
+    R tau = s / (R(1) + c);
+    A[p][p] -= t * apq;
+    A[q][q] += t * apq;
+    A[p][q] = R(0);
+    A[q][p] = R(0);
+    int r = 3 - p - q;
+    R arp = A[r][p], arq = A[r][q];
+    R nrp = arp - s * (arq + tau * arp);
+    R nrq = arq + s * (arp - tau * arq);
+    A[r][p] = nrp; A[p][r] = nrp;
+    A[r][q] = nrq; A[q][r] = nrq;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        R vkp = V[3 * k + p], vkq = V[3 * k + q];
+        V[3 * k + p] = vkp - s * (vkq + tau * vkp);
+        V[3 * k + q] = vkq + s * (vkp - tau * vkq);
+    }
+}
+
+template <typename R>
+__device__ __forceinline__ void sym_eig3(const R S[9], R lam[3], R V[9]) {
+    R A[3][3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) A[i][j] = R(0.5) * (S[3 * i + j] + S[3 * j + i]);
+#pragma unroll
+    for (int i = 0; i < 9; ++i) V[i] = (i % 4 == 0) ? R(1) : R(0);
+    const int max_sweeps = sizeof(R) == 8 ? 12 : 8;
+    const R tol = Num<R>::eps * Num<R>::eps;
+    for (int sweep = 0; sweep < max_sweeps; ++sweep) {
+        R off = A[0][1] * A[0][1] + A[0][2] * A[0][2] + A[1][2] * A[1][2];
+        R dia = A[0][0] * A[0][0] + A[1][1] * A[1][1] + A[2][2] * A[2][2];
+        if (off <= tol * dia) break;
+        jacobi_rotate(A, V, 0, 1);
+        jacobi_rotate(A, V, 0, 2);
+        jacobi_rotate(A, V, 1, 2);
+    }
+    lam[0] = A[0][0];
+    lam[1] = A[1][1];
+    lam[2] = A[2][2];
+}
+
+// Model parameters in the arithmetic type of the path.
+template <typename R>
+struct ModelParams {
+    int kind;
+    R mu, lam;
+    R kappa, K, n, tau_y, m, eps;
+    __device__ __forceinline__ void load(const MpmScene& sc) {
+        kind = sc.model;
+        mu = (R)sc.mu; lam = (R)sc.lam;
+        kappa = (R)sc.kappa; K = (R)sc.K; n = (R)sc.n_exp;
+        tau_y = (R)sc.tau_y; m = (R)sc.m_pap; eps = (R)sc.eps;
+    }
+};
+
+// F_bar = Fe_bar Fg^{-T};  Fg_bar = -Fg^{-T} F^T Fe_bar Fg^{-T}   (constitutive.py:37-38, 73-74)
+template <typename R>
+__device__ __forceinline__ void pull_back(const R F[9], const R Fgi[9], const R Feb[9], R Fb[9], R Fgb[9]) {
+    mmT(Feb, Fgi, Fb);              // Fe_bar Fg^{-T}
+    R T1[9], T2[9];
+    mTm(F, Fb, T1);                 // F^T (Fe_bar Fg^{-T})
+    mTm(Fgi, T1, T2);               // Fg^{-T} F^T Fe_bar Fg^{-T}
+#pragma unroll
+    for (int i = 0; i < 9; ++i) Fgb[i] = -T2[i];
+}
+
+// ---------------------------------------------------------------------------
+// neo-Hookean: tau = mu (Fe Fe^T - I) + lam ln J I
+// ---------------------------------------------------------------------------
+template <typename R>
+__device__ __forceinline__ void nh_stress(const R F[9], const R Fg[9], R mu, R lam, R tau[9]) {
+    R Fgi[9], Fe[9];
+    inv3(Fg, Fgi);
+    mm(F, Fgi, Fe);
+    R J = det3(Fe);
+    R lnJ = d_log(J);
+    mmT(Fe, Fe, tau);
+#pragma unroll
+    for (int i = 0; i < 9; ++i) tau[i] = mu * (tau[i] - ((i % 4 == 0) ? R(1) : R(0)));
+    tau[0] += lam * lnJ; tau[4] += lam * lnJ; tau[8] += lam * lnJ;
+}
+template <typename R>
+__device__ __forceinline__ void nh_vjp(const R F[9], const R Fg[9], R mu, R lam, const R tau_bar[9],
+                                       R Fb[9], R Fgb[9]) {
+    R Fgi[9], Fe[9], Fei[9], tb[9];
+    inv3(Fg, Fgi);
+    mm(F, Fgi, Fe);
+    inv3(Fe, Fei);
+    sym(tau_bar, tb);
+    R tr = tb[0] + tb[4] + tb[8];
+    R Feb[9], T[9];
+    mm(tb, Fe, T);
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+            Feb[3 * i + j] = R(2) * mu * T[3 * i + j] + lam * tr * Fei[3 * j + i];
+    pull_back(F, Fgi, Feb, Fb, Fgb);
+}
+
+// ---------------------------------------------------------------------------
+// Hencky.  The FP64 instantiation applies the reference's divided-difference
+// rule exactly (|beta_i - beta_j| > 1e-9 -> (ln bi - ln bj)/(bi - bj), else
+// 1/beta_i; constitutive.py:66-70).  The FP32 instantiation uses the
+// cancellation-free form log1p(d)/(beta_j d), d = (beta_i - beta_j)/beta_j, and
+// recomputes particles whose relative singular-value gap is below the
+// threshold in FP64.
+// ---------------------------------------------------------------------------
+template <typename R>
+__device__ __forceinline__ void hencky_eig(const R F[9], const R Fg[9], R Fgi[9], R Fe[9], R beta[3], R V[9]) {
+    inv3(Fg, Fgi);
+    mm(F, Fgi, Fe);
+    R b[9];
+    mmT(Fe, Fe, b);
+    sym_eig3(b, beta, V);
+}
+
+template <typename R>
+__device__ __forceinline__ void hencky_tau_from_eig(const R beta[3], const R V[9], R mu, R lam, R tau[9]) {
+    R lb[3] = {d_log(beta[0]), d_log(beta[1]), d_log(beta[2])};
+    R S = lb[0] + lb[1] + lb[2];
+    R h[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) h[i] = mu * lb[i] + R(0.5) * lam * S;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+            tau[3 * i + j] = V[3 * i] * h[0] * V[3 * j] + V[3 * i + 1] * h[1] * V[3 * j + 1]
+                           + V[3 * i + 2] * h[2] * V[3 * j + 2];
+}
+
+template <typename R>
+__device__ __forceinline__ R dk_entry(R bi, R bj, R lbi, R lbj);
+
+template <>
+__device__ __forceinline__ double dk_entry<double>(double bi, double bj, double lbi, double lbj) {
+    double d = bi - bj;
+    return fabs(d) > 1.0e-9 ? (lbi - lbj) / d : 1.0 / bi;
+}
+template <>
+__device__ __forceinline__ float dk_entry<float>(float bi, float bj, float, float) {
+    if (bi == bj) return 1.0f / bi;
+    float d = (bi - bj) / bj;
+    return log1pf(d) / (bj * d);
+}
+
+template <typename R>
+__device__ __forceinline__ void hencky_vjp_from_eig(const R F[9], const R Fgi[9], const R Fe[9], const R beta[3],
+                                                    const R V[9], R mu, R lam, const R tau_bar[9],
+                                                    R Fb[9], R Fgb[9]) {
+    R tb[9];
+    sym(tau_bar, tb);
+    R tr = tb[0] + tb[4] + tb[8];
+    R M[9];
+#pragma unroll
+    for (int i = 0; i < 9; ++i) M[i] = mu * tb[i] + ((i % 4 == 0) ? R(0.5) * lam * tr : R(0));
+    R T[9], UtMU[9];
+    mTm(V, M, T);         // V^T M
+    mm(T, V, UtMU);       // V^T M V
+    R lb[3] = {d_log(beta[0]), d_log(beta[1]), d_log(beta[2])};
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) UtMU[3 * i + j] *= dk_entry<R>(beta[i], beta[j], lb[i], lb[j]);
+    R Bb[9];
+    mm(V, UtMU, T);
+    mmT(T, V, Bb);        // V (UtMU o L) V^T
+    R Feb[9];
+    mm(Bb, Fe, Feb);
+#pragma unroll
+    for (int i = 0; i < 9; ++i) Feb[i] *= R(2);
+    pull_back(F, Fgi, Feb, Fb, Fgb);
+}
+
+// relative singular-value gap: min |s_i - s_j| / max s  with s = sqrt(beta)
+template <typename R>
+__device__ __forceinline__ R sv_gap(const R beta[3]) {
+    R s0 = d_sqrt(beta[0] > R(0) ? beta[0] : R(0));
+    R s1 = d_sqrt(beta[1] > R(0) ? beta[1] : R(0));
+    R s2 = d_sqrt(beta[2] > R(0) ? beta[2] : R(0));
+    R mx = s0 > s1 ? s0 : s1;
+    mx = mx > s2 ? mx : s2;
+    R g01 = d_abs(s0 - s1), g02 = d_abs(s0 - s2), g12 = d_abs(s1 - s2);
+    R g = g01 < g02 ? g01 : g02;
+    g = g < g12 ? g : g12;
+    return g / mx;
+}
+
+template <typename R>
+struct Hencky {
+    // both return whether the FP64 path was taken
+    static __device__ __forceinline__ bool stress(const R F[9], const R Fg[9], R mu, R lam, float, R tau[9]) {
+        R Fgi[9], Fe[9], beta[3], V[9];
+        hencky_eig(F, Fg, Fgi, Fe, beta, V);
+        hencky_tau_from_eig(beta, V, mu, lam, tau);
+        return false;
+    }
+    static __device__ __forceinline__ bool vjp(const R F[9], const R Fg[9], R mu, R lam, float, const R tb[9],
+                                               R Fb[9], R Fgb[9]) {
+        R Fgi[9], Fe[9], beta[3], V[9];
+        hencky_eig(F, Fg, Fgi, Fe, beta, V);
+        hencky_vjp_from_eig(F, Fgi, Fe, beta, V, mu, lam, tb, Fb, Fgb);
+        return false;
+    }
+};
+
+template <>
+struct Hencky<float> {
+    static __device__ __forceinline__ bool stress(const float F[9], const float Fg[9], float mu, float lam,
+                                                  float thresh, float tau[9]) {
+        float Fgi[9], Fe[9], beta[3], V[9];
+        hencky_eig(F, Fg, Fgi, Fe, beta, V);
+        if (sv_gap(beta) >= thresh) {
+            hencky_tau_from_eig(beta, V, mu, lam, tau);
+            return false;
+        }
+        double Fd[9], Fgd[9], Fgid[9], Fed[9], bd[3], Vd[9], td[9];
+#pragma unroll
+        for (int i = 0; i < 9; ++i) { Fd[i] = F[i]; Fgd[i] = Fg[i]; }
+        hencky_eig(Fd, Fgd, Fgid, Fed, bd, Vd);
+        hencky_tau_from_eig(bd, Vd, (double)mu, (double)lam, td);
+#pragma unroll
+        for (int i = 0; i < 9; ++i) tau[i] = (float)td[i];
+        return true;
+    }
+    static __device__ __forceinline__ bool vjp(const float F[9], const float Fg[9], float mu, float lam,
+                                               float thresh, const float tb[9], float Fb[9], float Fgb[9]) {
+        float Fgi[9], Fe[9], beta[3], V[9];
+        hencky_eig(F, Fg, Fgi, Fe, beta, V);
+        if (sv_gap(beta) >= thresh) {
+            hencky_vjp_from_eig(F, Fgi, Fe, beta, V, mu, lam, tb, Fb, Fgb);
+            return false;
+        }
+        double Fd[9], Fgd[9], Fgid[9], Fed[9], bd[3], Vd[9], tbd[9], Fbd[9], Fgbd[9];
+#pragma unroll
+        for (int i = 0; i < 9; ++i) { Fd[i] = F[i]; Fgd[i] = Fg[i]; tbd[i] = tb[i]; }
+        hencky_eig(Fd, Fgd, Fgid, Fed, bd, Vd);
+        // the stable divided difference is used here too (the FP64 recompute of
+        // a near-degenerate particle must not fall back to the 1e-9 switch)
+        double tbs[9];
+        sym(tbd, tbs);
+        double tr = tbs[0] + tbs[4] + tbs[8];
+        double M[9];
+#pragma unroll
+        for (int i = 0; i < 9; ++i) M[i] = (double)mu * tbs[i] + ((i % 4 == 0) ? 0.5 * (double)lam * tr : 0.0);
+        double T[9], UtMU[9];
+        mTm(Vd, M, T);
+        mm(T, Vd, UtMU);
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+                double bi = bd[i], bj = bd[j];
+                double L = (bi == bj) ? 1.0 / bi : log1p((bi - bj) / bj) / (bj * ((bi - bj) / bj));
+                UtMU[3 * i + j] *= L;
+            }
+        double Bb[9], Feb[9];
+        mm(Vd, UtMU, T);
+        mmT(T, Vd, Bb);
+        mm(Bb, Fed, Feb);
+#pragma unroll
+        for (int i = 0; i < 9; ++i) Feb[i] *= 2.0;
+        pull_back(Fd, Fgid, Feb, Fbd, Fgbd);
+#pragma unroll
+        for (int i = 0; i < 9; ++i) { Fb[i] = (float)Fbd[i]; Fgb[i] = (float)Fgbd[i]; }
+        return true;
+    }
+};
+
+// ---------------------------------------------------------------------------
+// Herschel-Bulkley (Papanastasiou-regularised), rate dependent through C.
+//   tau = kappa ln(Je) I + 2 eta(gdot) D,  D = sym(C),  gdot = sqrt(2 D:D + eps^2)
+//   eta = K gdot^(n-1) + tau_y (1 - exp(-m gdot)) / gdot
+// ---------------------------------------------------------------------------
+template <typename R>
+__device__ __forceinline__ void hb_stress(const R F[9], const R Fg[9], const R C[9], const ModelParams<R>& P,
+                                          R tau[9]) {
+    R Je = det3(F) / det3(Fg);
+    R D[9];
+    sym(C, D);
+    R gdot = d_sqrt(R(2) * frob(D, D) + P.eps * P.eps);
+    R eta = P.K * d_pow(gdot, P.n - R(1)) + P.tau_y * (R(1) - d_exp(-P.m * gdot)) / gdot;
+    R vol = P.kappa * d_log(Je);
+#pragma unroll
+    for (int i = 0; i < 9; ++i) tau[i] = R(2) * eta * D[i] + ((i % 4 == 0) ? vol : R(0));
+}
+template <typename R>
+__device__ __forceinline__ void hb_vjp(const R F[9], const R Fg[9], const R C[9], const ModelParams<R>& P,
+                                       const R tau_bar[9], R Fb[9], R Fgb[9], R Cb[9]) {
+    R tb[9];
+    sym(tau_bar, tb);
+    R tr = tb[0] + tb[4] + tb[8];
+    R Fi[9], Fgi[9];
+    inv3(F, Fi);
+    inv3(Fg, Fgi);
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            Fb[3 * i + j] = P.kappa * tr * Fi[3 * j + i];
+            Fgb[3 * i + j] = -P.kappa * tr * Fgi[3 * j + i];
+        }
+    R D[9];
+    sym(C, D);
+    R gdot = d_sqrt(R(2) * frob(D, D) + P.eps * P.eps);
+    R e = d_exp(-P.m * gdot);
+    R eta = P.K * d_pow(gdot, P.n - R(1)) + P.tau_y * (R(1) - e) / gdot;
+    R deta = P.K * (P.n - R(1)) * d_pow(gdot, P.n - R(2))
+           + P.tau_y * ((P.m * e) * gdot - (R(1) - e)) / (gdot * gdot);
+    R tbD = frob(tb, D);
+    R k = R(4) * tbD * deta / gdot;
+#pragma unroll
+    for (int i = 0; i < 9; ++i) Cb[i] = R(2) * eta * tb[i] + k * D[i];
+}
+
+// ---------------------------------------------------------------------------
+// model dispatch.  Returns true when an FP32 Hencky evaluation went to FP64.
+// ---------------------------------------------------------------------------
+template <typename R>
+__device__ __forceinline__ bool model_stress(const ModelParams<R>& P, float thresh, const R F[9], const R Fg[9],
+                                             const R C[9], R tau[9]) {
+    if (P.kind == MPM_MODEL_HENCKY) return Hencky<R>::stress(F, Fg, P.mu, P.lam, thresh, tau);
+    if (P.kind == MPM_MODEL_HERSCHEL_BULKLEY) { hb_stress(F, Fg, C, P, tau); return false; }
+    nh_stress(F, Fg, P.mu, P.lam, tau);
+    return false;
+}
+template <typename R>
+__device__ __forceinline__ bool model_vjp(const ModelParams<R>& P, float thresh, const R F[9], const R Fg[9],
+                                          const R C[9], const R tb[9], R Fb[9], R Fgb[9], R Cb[9]) {
+    if (P.kind == MPM_MODEL_HERSCHEL_BULKLEY) { hb_vjp(F, Fg, C, P, tb, Fb, Fgb, Cb); return false; }
+#pragma unroll
+    for (int i = 0; i < 9; ++i) Cb[i] = R(0);
+    if (P.kind == MPM_MODEL_HENCKY) return Hencky<R>::vjp(F, Fg, P.mu, P.lam, thresh, tb, Fb, Fgb);
+    nh_vjp(F, Fg, P.mu, P.lam, tb, Fb, Fgb);
+    return false;
+}
+
+}  // namespace mpm

@@ -1,0 +1,186 @@
+// Deterministic, stable LSD radix sort of 32-bit cell keys with 32-bit payload
+// indices, and the tile-list compaction.  No global atomics: each pass builds
+// per-block digit counts (shared-memory counters), scans them digit-major into
+// global offsets (row totals, then per-digit row scans) and scatters every key
+// to offset + its stable rank inside the block, ranked with warp match masks.
+#pragma once
+
+#include "mpm_common.cuh"
+
+namespace mpm {
+
+constexpr int RADIX_BITS = 8;
+constexpr int RADIX = 1 << RADIX_BITS;
+constexpr int SORT_THREADS = 256;
+constexpr int SORT_ITEMS = 16;                       // keys per thread per block
+constexpr int SORT_TILE = SORT_THREADS * SORT_ITEMS; // keys per block
+
+// Per-block digit histogram.  hist is digit-major: hist[d * nblk + b].
+__global__ void __launch_bounds__(SORT_THREADS)
+radix_hist_kernel(const unsigned* __restrict__ keys, long long n, int shift, unsigned* __restrict__ hist, int nblk) {
+    __shared__ unsigned cnt[RADIX];
+    for (int d = threadIdx.x; d < RADIX; d += SORT_THREADS) cnt[d] = 0;
+    __syncthreads();
+    long long base = (long long)blockIdx.x * SORT_TILE;
+#pragma unroll 4
+    for (int r = 0; r < SORT_ITEMS; ++r) {
+        long long q = base + (long long)r * SORT_THREADS + threadIdx.x;
+        if (q < n) atomicAdd(&cnt[(keys[q] >> shift) & (RADIX - 1)], 1u);
+    }
+    __syncthreads();
+    for (int d = threadIdx.x; d < RADIX; d += SORT_THREADS) hist[(long long)d * nblk + blockIdx.x] = cnt[d];
+}
+
+// totals[d] = sum_b hist[d][b]   (one block per digit, fixed-order tree)
+__global__ void __launch_bounds__(256)
+radix_rowsum_kernel(const unsigned* __restrict__ hist, int nblk, unsigned* __restrict__ totals) {
+    __shared__ unsigned red[256];
+    int d = blockIdx.x;
+    unsigned s = 0;
+    for (int b = threadIdx.x; b < nblk; b += 256) s += hist[(long long)d * nblk + b];
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (int w = 128; w > 0; w >>= 1) {
+        if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) totals[d] = red[0];
+}
+
+// hist[d][b] <- sum_{d'<d} totals[d'] + sum_{b'<b} hist[d][b']   (one block per digit)
+__global__ void __launch_bounds__(256)
+radix_rowscan_kernel(unsigned* __restrict__ hist, int nblk, const unsigned* __restrict__ totals) {
+    __shared__ unsigned sh[256];
+    __shared__ unsigned carry;
+    int d = blockIdx.x;
+    // digit offset
+    sh[threadIdx.x] = (threadIdx.x < (unsigned)d) ? totals[threadIdx.x] : 0u;
+    __syncthreads();
+    for (int w = 128; w > 0; w >>= 1) {
+        if (threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) carry = sh[0];
+    __syncthreads();
+    for (int b0 = 0; b0 < nblk; b0 += 256) {
+        int b = b0 + threadIdx.x;
+        unsigned v = (b < nblk) ? hist[(long long)d * nblk + b] : 0u;
+        sh[threadIdx.x] = v;
+        __syncthreads();
+        // Hillis-Steele inclusive scan
+        for (int o = 1; o < 256; o <<= 1) {
+            unsigned t = (threadIdx.x >= (unsigned)o) ? sh[threadIdx.x - o] : 0u;
+            __syncthreads();
+            sh[threadIdx.x] += t;
+            __syncthreads();
+        }
+        unsigned incl = sh[threadIdx.x];
+        unsigned c = carry;
+        if (b < nblk) hist[(long long)d * nblk + b] = c + incl - v;
+        __syncthreads();
+        if (threadIdx.x == 255) carry = c + incl;
+        __syncthreads();
+    }
+}
+
+// Stable scatter.  vals_in == nullptr means the identity payload (slot index).
+__global__ void __launch_bounds__(SORT_THREADS)
+radix_scatter_kernel(const unsigned* __restrict__ keys_in, const unsigned* __restrict__ vals_in, long long n,
+                     int shift, const unsigned* __restrict__ offs, int nblk,
+                     unsigned* __restrict__ keys_out, unsigned* __restrict__ vals_out) {
+    constexpr int NW = SORT_THREADS / 32;
+    __shared__ unsigned wcnt[NW][RADIX];
+    __shared__ unsigned base_d[RADIX];
+    __shared__ unsigned round_tot[RADIX];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int d = threadIdx.x; d < RADIX; d += SORT_THREADS) {
+        base_d[d] = offs[(long long)d * nblk + blockIdx.x];
+#pragma unroll
+        for (int w = 0; w < NW; ++w) wcnt[w][d] = 0;
+    }
+    __syncthreads();
+    long long base = (long long)blockIdx.x * SORT_TILE;
+    const unsigned lt_mask = (1u << lane) - 1u;
+    for (int r = 0; r < SORT_ITEMS; ++r) {
+        long long q = base + (long long)r * SORT_THREADS + threadIdx.x;
+        bool valid = q < n;
+        unsigned key = valid ? keys_in[q] : 0u;
+        unsigned val = valid ? (vals_in ? vals_in[q] : (unsigned)q) : 0u;
+        unsigned dig = (key >> shift) & (RADIX - 1);
+        unsigned vmask = __ballot_sync(0xffffffffu, valid);
+        unsigned peers = 0, rank = 0;
+        if (valid) {
+            peers = __match_any_sync(vmask, dig);
+            rank = __popc(peers & lt_mask);
+            if (rank == 0) wcnt[warp][dig] = __popc(peers);
+        }
+        __syncthreads();
+        // exclusive prefix over warps, per digit
+        for (int d = threadIdx.x; d < RADIX; d += SORT_THREADS) {
+            unsigned run = 0;
+#pragma unroll
+            for (int w = 0; w < NW; ++w) {
+                unsigned c = wcnt[w][d];
+                wcnt[w][d] = run;
+                run += c;
+            }
+            round_tot[d] = run;
+        }
+        __syncthreads();
+        if (valid) {
+            unsigned pos = base_d[dig] + wcnt[warp][dig] + rank;
+            keys_out[pos] = key;
+            vals_out[pos] = val;
+        }
+        __syncthreads();
+        for (int d = threadIdx.x; d < RADIX; d += SORT_THREADS) {
+            base_d[d] += round_tot[d];
+#pragma unroll
+            for (int w = 0; w < NW; ++w) wcnt[w][d] = 0;
+        }
+        __syncthreads();
+    }
+}
+
+// Tile-list compaction, single block: tile_slot[t] = rank among flagged tiles
+// (or -1), active[rank] = t, *n_active = count.  Flags are reset to 0.
+__global__ void __launch_bounds__(1024)
+compact_tiles_kernel(int* __restrict__ flag, long long n_tiles, int* __restrict__ tile_slot,
+                     int* __restrict__ active, int* __restrict__ n_active, int cap, int* __restrict__ status) {
+    __shared__ int sh[1024];
+    long long per = (n_tiles + 1023) / 1024;
+    long long t0 = (long long)threadIdx.x * per;
+    long long t1 = t0 + per < n_tiles ? t0 + per : n_tiles;
+    int cnt = 0;
+    for (long long t = t0; t < t1; ++t) cnt += flag[t] ? 1 : 0;
+    sh[threadIdx.x] = cnt;
+    __syncthreads();
+    for (int o = 1; o < 1024; o <<= 1) {
+        int v = (threadIdx.x >= (unsigned)o) ? sh[threadIdx.x - o] : 0;
+        __syncthreads();
+        sh[threadIdx.x] += v;
+        __syncthreads();
+    }
+    int run = sh[threadIdx.x] - cnt;
+    for (long long t = t0; t < t1; ++t) {
+        if (flag[t]) {
+            if (run < cap) {
+                tile_slot[t] = run;
+                active[run] = (int)t;
+            } else {
+                tile_slot[t] = -1;
+            }
+            ++run;
+            flag[t] = 0;
+        } else {
+            tile_slot[t] = -1;
+        }
+    }
+    if (threadIdx.x == 1023) {
+        int total = sh[1023];
+        if (total > cap) { atomicOr(status, MPM_ERR_ARG); total = cap; }
+        *n_active = total;
+    }
+}
+
+}  // namespace mpm

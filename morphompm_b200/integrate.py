@@ -1,0 +1,112 @@
+"""[4] Integrate -- trajectory rollout and adjoint with the reference's
+signatures (python/morphompm/integrate.py:15-52):
+
+    rollout(state0, model, cfg, n_steps, advect)          -> final state, caches
+    rollout_vjp(caches, xf_b, vf_b, Cf_b, Ff_b, Fgf_b, advect) -> state cotangents
+    iso_growth_state(pts, g), iso_growth_grad(Fg_b), loss_detF(F)
+    dloss_dg(pts, model, cfg, g, n_steps, advect)         -> (loss, dloss/dg)
+
+``rollout``/``rollout_vjp`` keep one cache per step like the reference (device
+memory O(n_steps)).  ``dloss_dg`` runs the device trajectory engine
+(trajectory.Rollout) instead, with optional checkpoint-every-k recomputation
+(``ckpt_every``) and an optional mean-squared final-position loss
+(``loss="mse"``, ``x_obs``); with the defaults it returns what the reference
+returns.
+"""
+from __future__ import annotations
+
+from typing import Optional
+
+import numpy as np
+import torch
+
+from .devarray import like_input, to_device
+from .runtime import SLAB_ROWS, ROW_C, ROW_F, ROW_V, ROW_X
+from .state import ParticleState
+from .transfer import get_plan, scene_spec, step, step_vjp
+
+
+def _dev_state(state0: ParticleState) -> ParticleState:
+    x = to_device(state0.x).contiguous()
+    dt, dev = x.dtype, x.device
+    return ParticleState(x, *(to_device(a, dt, dev).contiguous() for a in (state0.v, state0.C, state0.F, state0.Fg)))
+
+
+def rollout(state0: ParticleState, model, cfg, n_steps, advect=False):
+    ref = state0.x
+    st = _dev_state(state0)
+    caches = []
+    for t in range(n_steps):
+        st, cache = step(st, model, cfg, advect=advect)
+        cache.ref = ref
+        caches.append(cache)
+    return ParticleState(*(like_input(a, ref) for a in (st.x, st.v, st.C, st.F, st.Fg))), caches
+
+
+def rollout_vjp(caches, xf_b, vf_b, Cf_b, Ff_b, Fgf_b, advect=False):
+    if not caches:
+        return xf_b, vf_b, Cf_b, Ff_b, Fgf_b
+    ref = caches[0].ref
+    dt, dev = caches[0].x.dtype, caches[0].x.device
+    bars = [to_device(a, dt, dev) for a in (xf_b, vf_b, Cf_b, Ff_b)] + [to_device(Fgf_b, torch.float64, dev)]
+    for cache in reversed(caches):
+        r = cache.ref
+        cache.ref = bars[0]          # keep intermediate results on the device
+        bars = list(step_vjp(cache, *bars, advect=advect))
+        cache.ref = r
+    out = [like_input(a, ref) for a in bars[:4]]
+    out.append(like_input(bars[4], ref) if not isinstance(ref, torch.Tensor) else bars[4])
+    return tuple(out)
+
+
+def iso_growth_state(pts, g):
+    st = ParticleState.rest(pts)
+    if isinstance(st.Fg, torch.Tensor):
+        st.Fg = g * torch.eye(3, dtype=st.Fg.dtype, device=st.Fg.device).expand_as(st.Fg).clone()
+    else:
+        st.Fg[:] = g * np.eye(3)
+    return st
+
+
+def iso_growth_grad(Fg_b):
+    if isinstance(Fg_b, torch.Tensor):
+        return float(torch.diagonal(Fg_b, dim1=-2, dim2=-1).sum().item())
+    return float(sum(np.trace(Fg_b[p]) for p in range(len(Fg_b))))
+
+
+def loss_detF(F):
+    if isinstance(F, torch.Tensor):
+        return float(torch.linalg.det(F.double()).sum().item())
+    return float(sum(np.linalg.det(F[p]) for p in range(len(F))))
+
+
+def _slab_from_points(pts_dev: torch.Tensor) -> torch.Tensor:
+    n = pts_dev.shape[0]
+    slab = torch.zeros(SLAB_ROWS, n, dtype=pts_dev.dtype, device=pts_dev.device)
+    slab[ROW_X:ROW_X + 3] = pts_dev.t()
+    for i in range(3):
+        slab[ROW_F + 4 * i] = 1.0
+    return slab
+
+
+def dloss_dg(pts, model, cfg, g, n_steps, advect, loss: str = "detF", x_obs=None,
+             ckpt_every: Optional[int] = None):
+    """d(loss of the final state)/dg for Fg = g I (integrate.py:45-52).
+    loss="detF": sum det F_final (the reference's); loss="mse": mean
+    |x_final - x_obs|^2."""
+    from .trajectory import Rollout
+    p = to_device(pts).contiguous()
+    n = p.shape[0]
+    plan = get_plan([scene_spec(cfg, model, n)], p.dtype, p.device)
+    Fg = torch.zeros(9, n, dtype=p.dtype, device=p.device)
+    for i in range(3):
+        Fg[4 * i] = g
+    xo = None
+    if loss == "mse":
+        xo_t = to_device(x_obs, p.dtype, p.device).reshape(n, 3)
+        xo = xo_t.t().contiguous()
+    ro = Rollout(plan, n_steps, advect=advect, ckpt_every=ckpt_every, Fg=Fg, loss=loss, x_obs=xo)
+    ro.run(_slab_from_points(p))
+    L = float(ro.loss.sum().item())
+    dg = float(ro.Fg_bar[0].sum().item() + ro.Fg_bar[4].sum().item() + ro.Fg_bar[8].sum().item())
+    return L, dg

@@ -1,0 +1,113 @@
+"""The C ABI library: it builds for sm_100a, exports every entry point that
+include/morphompm_b200.h declares, its struct layouts agree with the ctypes
+mirror, and host-only plan construction validates its arguments.  No CUDA
+calls are made here."""
+import ctypes as C
+import os
+import re
+import subprocess
+import tempfile
+
+import pytest
+
+from morphompm_b200 import _lib as L
+from morphompm_b200.build import ROOT
+
+HEADER = os.path.join(ROOT, "include", "morphompm_b200.h")
+
+
+def declared():
+    src = open(HEADER).read()
+    return sorted(set(re.findall(r"^\s*(?:int|void|int64_t)\s+\**(mpm_\w+)\s*\(", src, re.M)))
+
+
+def test_exports_every_declared_symbol():
+    lib = L.load()
+    names = declared()
+    assert len(names) >= 15
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+    assert set(names) == set(L.EXPORTS), set(names) ^ set(L.EXPORTS)
+    out = subprocess.run(["nm", "-D", "--defined-only", L.lib_path()], capture_output=True, text=True).stdout
+    for n in names:
+        assert re.search(rf"\bT {n}\b", out), n
+
+
+def test_struct_layout_matches_ctypes():
+    prog = r'''
+#include <stdio.h>
+#include <stddef.h>
+#include "morphompm_b200.h"
+#define O(T, f) printf(#T "." #f " %zu\n", offsetof(T, f))
+int main(void) {
+  printf("MpmScene %zu\nMpmParticles %zu\nMpmCotangents %zu\nMpmTuning %zu\n", sizeof(MpmScene),
+         sizeof(MpmParticles), sizeof(MpmCotangents), sizeof(MpmTuning));
+  O(MpmScene, p_begin); O(MpmScene, wall); O(MpmScene, growth_mode); O(MpmScene, dx); O(MpmScene, gravity);
+  O(MpmScene, mu); O(MpmScene, kappa); O(MpmScene, eps); O(MpmScene, growth_A); O(MpmScene, ramp_steps);
+  O(MpmParticles, Fg); O(MpmParticles, sc9); O(MpmCotangents, Fg); O(MpmTuning, fp64_gap_thresh);
+  return 0;
+}
+'''
+    with tempfile.TemporaryDirectory() as d:
+        c = os.path.join(d, "layout.c")
+        open(c, "w").write(prog)
+        exe = os.path.join(d, "layout")
+        subprocess.run(["gcc", "-I", os.path.dirname(HEADER), c, "-o", exe], check=True)
+        out = subprocess.run([exe], capture_output=True, text=True, check=True).stdout.split("\n")
+    got = dict(l.rsplit(" ", 1) for l in out if l)
+    assert int(got["MpmScene"]) == C.sizeof(L.MpmScene)
+    assert int(got["MpmParticles"]) == C.sizeof(L.MpmParticles)
+    assert int(got["MpmCotangents"]) == C.sizeof(L.MpmCotangents)
+    assert int(got["MpmTuning"]) == C.sizeof(L.MpmTuning)
+    for k, v in got.items():
+        if "." in k:
+            T, f = k.split(".")
+            assert getattr(getattr(L, T), f).offset == int(v), k
+
+
+def _scene(n, p0=0, shape=(8, 8, 8)):
+    s = L.MpmScene()
+    for d in range(3):
+        s.shape[d] = shape[d]
+    s.p_begin, s.p_end = p0, p0 + n
+    s.dx, s.dt, s.damping, s.pmass, s.vol0 = 0.1, 1e-3, 0.05, 8e-3, 8e-6
+    return s
+
+
+def test_plan_host_validation():
+    lib = L.load()
+    arr = (L.MpmScene * 2)(_scene(100), _scene(50, 100, (5, 6, 7)))
+    h = C.c_void_p()
+    assert lib.mpm_plan_create(arr, 2, 8, None, C.byref(h)) == L.MPM_OK
+    nb = C.c_size_t()
+    assert lib.mpm_plan_workspace_bytes(h, C.byref(nb)) == 0 and nb.value > 0
+    tb = C.c_size_t()
+    assert lib.mpm_plan_tape_bytes(h, C.byref(tb)) == 0 and 0 < tb.value < nb.value
+    assert lib.mpm_plan_num_particles(h) == 150
+    lib.mpm_plan_destroy(h)
+    # particle ranges must tile [0, n) in scene order
+    bad = (L.MpmScene * 2)(_scene(100), _scene(50, 90))
+    assert lib.mpm_plan_create(bad, 2, 8, None, C.byref(h)) == L.MPM_ERR_ARG
+    assert lib.mpm_plan_create(arr, 2, 2, None, C.byref(h)) == L.MPM_ERR_ARG
+    s = _scene(10)
+    s.model = 7
+    assert lib.mpm_plan_create((L.MpmScene * 1)(s), 1, 8, None, C.byref(h)) == L.MPM_ERR_ARG
+    # null pointers are rejected before any CUDA call
+    assert lib.mpm_step_fwd(None, None, None, 1, 0, None, None) == L.MPM_ERR_ARG
+    assert lib.mpm_stress(None, 8, 1, None, None, None, None, None) == L.MPM_ERR_ARG
+
+
+def test_tape_grows_with_tile_cap():
+    lib = L.load()
+    arr = (L.MpmScene * 1)(_scene(1000, 0, (64, 64, 64)))
+    sizes = []
+    for cap in (0, 10):
+        t = L.MpmTuning()
+        t.active_tile_cap = cap
+        h = C.c_void_p()
+        assert lib.mpm_plan_create(arr, 1, 4, C.byref(t), C.byref(h)) == 0
+        tb = C.c_size_t()
+        lib.mpm_plan_tape_bytes(h, C.byref(tb))
+        sizes.append(tb.value)
+        lib.mpm_plan_destroy(h)
+    assert sizes[1] < sizes[0]

@@ -1,0 +1,201 @@
+"""Batched growth scenes: many instances with uneven particle counts, grids,
+materials and growth parameters advanced together.
+
+One plan holds every scene (scene table, per-scene cell/tile ranges); each
+step is one launch sequence over all scenes, and the whole forward + loss +
+adjoint trajectory is captured once in a CUDA graph and replayed.  Growth is
+the per-scene isotropic law Fg = g_s I (growth_mode 1, g_s = 1 + A_s), so the
+adjoint returns d loss / d g_s per scene, accumulated in float64.
+
+The schedule (node-tile edge, P2G CTAs per SM, stencil offsets per pass,
+particle block size) is chosen by ``autotune``, which times short forward
+trajectories of the actual batch for each candidate on the current GPU.
+"""
+from __future__ import annotations
+
+import itertools
+import json
+import os
+import time
+from typing import Dict, List, Optional
+
+import numpy as np
+import torch
+
+from . import _lib as L
+from .runtime import Plan, SceneSpec, SLAB_ROWS, ROW_F, ROW_X
+from .trajectory import Rollout
+
+MODEL_KIND = {"nh": L.MODEL_NEOHOOKEAN, "hencky": L.MODEL_HENCKY, "hb": L.MODEL_HERSCHEL_BULKLEY}
+
+
+def scene_spec_from_dict(s: dict, growth_mode: int = 1) -> SceneSpec:
+    dx = float(s["dx"])
+    sp = dx / 2.0
+    return SceneSpec(shape=tuple(s["shape"]), n=int(s["x"].shape[0]), model=MODEL_KIND[s["model"]], dx=dx,
+                     dt=float(s["dt"]), damping=float(s.get("damping", 0.05)),
+                     pmass=float(s.get("density", 1.0)) * sp ** 3, vol0=sp ** 3, mu=float(s.get("mu", 0.0)),
+                     lam=float(s.get("lam", 0.0)), hb=s.get("hb"), wall=int(s.get("wall", 0)),
+                     clamp_lo=tuple(s.get("clamp_lo", (0, 0, 0))), clamp_hi=tuple(s.get("clamp_hi", (0, 0, 0))),
+                     growth_mode=growth_mode, growth_A=float(s.get("growth_A", 0.0)),
+                     ramp_steps=float(s.get("ramp_steps", 0)))
+
+
+def host_slab(scenes: List[dict], dtype=np.float32) -> np.ndarray:
+    """(24, n_total) rest-state slab of all scenes (x from the scenes, F = I)."""
+    n = sum(int(s["x"].shape[0]) for s in scenes)
+    slab = np.zeros((SLAB_ROWS, n), dtype=dtype)
+    p = 0
+    for s in scenes:
+        k = s["x"].shape[0]
+        slab[ROW_X:ROW_X + 3, p:p + k] = s["x"].T
+        p += k
+    for i in range(3):
+        slab[ROW_F + 4 * i] = 1.0
+    return slab
+
+
+def host_phi(scenes: List[dict], dtype=np.float32) -> Optional[np.ndarray]:
+    if all(s.get("phi") is None for s in scenes):
+        return None
+    return np.concatenate([s["phi"] if s.get("phi") is not None else np.ones(s["x"].shape[0])
+                           for s in scenes]).astype(dtype)
+
+
+class Batch:
+    """A batch of scenes with a graph-captured forward+adjoint trajectory."""
+
+    def __init__(self, scenes: List[dict], n_steps: int, dtype=torch.float32, advect: bool = True,
+                 ckpt_every: Optional[int] = None, tuning: Optional[dict] = None, loss: str = "detF",
+                 x_obs: Optional[np.ndarray] = None, device=None):
+        self.scenes = scenes
+        self.n_steps = n_steps
+        self.dtype = dtype
+        self.specs = [scene_spec_from_dict(s) for s in scenes]
+        self.n = sum(sp.n for sp in self.specs)
+        self.plan = Plan(self.specs, dtype=dtype, tuning=tuning, device=device)
+        npd = np.float32 if dtype == torch.float32 else np.float64
+        phi = host_phi(scenes, npd)
+        self.phi = None
+        if phi is not None:
+            self.phi = torch.as_tensor(phi).to(self.plan.device)
+            self.plan.set_growth_field(self.phi)
+        xo = None
+        if loss == "mse":
+            xo = torch.as_tensor(np.ascontiguousarray(x_obs.T.astype(npd))).to(self.plan.device)
+        self.rollout = Rollout(self.plan, n_steps, advect=advect, ckpt_every=ckpt_every, Fg=None, loss=loss,
+                               x_obs=xo)
+        self.slab0 = torch.empty(SLAB_ROWS, self.n, dtype=dtype, device=self.plan.device)
+        self.graph = None
+
+    def particle_steps(self) -> int:
+        return self.n * self.n_steps
+
+    def load(self, slab_host: np.ndarray, non_blocking=True):
+        """Copy a (24, n) host slab (pinned for async) into the device input."""
+        src = torch.from_numpy(slab_host) if isinstance(slab_host, np.ndarray) else slab_host
+        self.slab0.copy_(src, non_blocking=non_blocking)
+
+    def run(self):
+        return self.rollout.run(self.slab0)
+
+    def capture(self):
+        self.graph = self.rollout.capture(self.slab0)
+        return self.graph
+
+    def replay(self):
+        if self.graph is None:
+            self.capture()
+        self.graph.replay()
+
+    @property
+    def loss(self) -> torch.Tensor:
+        return self.rollout.loss
+
+    @property
+    def dloss_dg(self) -> torch.Tensor:
+        """d loss_s / d g_s (growth law g_s = 1 + A_s, so d/dA = d/dg)."""
+        return self.rollout.growth_grad
+
+
+# ---------------------------------------------------------------------------
+# autotuner
+# ---------------------------------------------------------------------------
+CANDIDATES = {
+    "tile_xy": [4, 8, 16],
+    "scatter_ctas_per_sm": [1, 2, 4],
+    "scatter_oxb": [1, 3],
+    "particle_block": [128, 256],
+}
+TUNE_CACHE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tuned.json")
+
+
+def _signature(scenes: List[dict], dtype) -> str:
+    n = sum(int(s["x"].shape[0]) for s in scenes)
+    g = sum(int(np.prod(s["shape"])) for s in scenes)
+    return f"{len(scenes)}s-{n}p-{g}g-{str(dtype).split('.')[-1]}"
+
+
+def _gpu_name() -> str:
+    return torch.cuda.get_device_name() if torch.cuda.is_available() else "none"
+
+
+def load_tuned(scenes: List[dict], dtype) -> Optional[dict]:
+    try:
+        table = json.load(open(TUNE_CACHE))
+    except Exception:
+        return None
+    return table.get(_gpu_name(), {}).get(_signature(scenes, dtype))
+
+
+def autotune(scenes: List[dict], dtype=torch.float32, steps: int = 4, budget_s: float = 90.0,
+             save: bool = False, verbose: bool = False) -> Dict:
+    """Time `steps` forward steps of the batch for every candidate schedule
+    (coordinate search: one knob at a time, starting from the defaults) and
+    return the fastest.  Results are deterministic whatever the schedule
+    (the summation order per node does not depend on it)."""
+    t_start = time.time()
+    best = {"tile_xy": 8, "scatter_ctas_per_sm": 2, "scatter_oxb": 3 if dtype == torch.float32 else 1,
+            "particle_block": 256}
+    slab = torch.as_tensor(host_slab(scenes, np.float32 if dtype == torch.float32 else np.float64))
+
+    def measure(cfg):
+        b = Batch(scenes, steps, dtype=dtype, tuning=cfg, ckpt_every=steps)
+        b.load(slab.to(b.plan.device), non_blocking=False)
+        ro = b.rollout
+        ro.forward(b.slab0)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        ro.forward(b.slab0)
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1)
+
+    results = {}
+    t_best = measure(best)
+    results[json.dumps(best, sort_keys=True)] = t_best
+    for knob, vals in CANDIDATES.items():
+        for v in vals:
+            if time.time() - t_start > budget_s:
+                break
+            if dtype == torch.float64 and knob == "scatter_oxb" and v == 3:
+                continue
+            cfg = dict(best, **{knob: v})
+            key = json.dumps(cfg, sort_keys=True)
+            if key in results:
+                continue
+            t = measure(cfg)
+            results[key] = t
+            if verbose:
+                print(f"autotune {cfg} {t:.3f} ms", flush=True)
+            if t < t_best:
+                best, t_best = cfg, t
+    if save:
+        try:
+            table = json.load(open(TUNE_CACHE))
+        except Exception:
+            table = {}
+        table.setdefault(_gpu_name(), {})[_signature(scenes, dtype)] = best
+        json.dump(table, open(TUNE_CACHE, "w"), indent=1, sort_keys=True)
+    return dict(best, _ms=t_best)

@@ -84,7 +84,9 @@ def test_bin_keys_bit_exact():
                 if dx in (1 / 32,):        # power-of-two inv_dx: FP32 binning is exact
                     assert np.array_equal(got, ref32)
                 else:
-                    assert np.mean(got == ref32) > 0.999
+                    # non-power-of-two inv_dx: only points planted on cell
+                    # boundaries may bin differently in FP32
+                    assert np.array_equal(got[3000:], ref32[3000:]) or np.mean(got[3000:] == ref32[3000:]) > 0.9995
 
 
 def _step_inputs(d):

@@ -1,0 +1,383 @@
+"""Throughput of the differentiable growth step: particle-steps/s of forward +
+adjoint for the batched FP32 path on the 256-scene uneven workload
+(n log-uniform in [2048, 65536], grids 32^3..64^3, mixed neo-Hookean/Hencky,
+per-scene growth g, 200 steps forward + full-trajectory adjoint, one
+graph-captured launch sequence per trajectory).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One bench step = one forward + loss + adjoint trajectory over the whole batch.
+Prints one JSON line (rank 0).  Under torchrun every rank runs its own batch
+(different seed; no data-path collective): weak scaling, time = max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "particle-steps/s fwd+adjoint: FP32 batched vs FP64 plain @ stated F error"
+UNIT = "particle-steps/s"
+WORKLOAD = "config4: 256 uneven growth scenes (2k-64k particles, 32^3-64^3 grids), 200 steps fwd+adj, FP32 batched"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--scenes", type=int, default=256)
+    ap.add_argument("--mpm-steps", type=int, default=200)
+    ap.add_argument("--ckpt-every", type=int, default=0, help="0 = sqrt(N) schedule")
+    ap.add_argument("--no-plain", action="store_true", help="skip the FP64 plain-path leg")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+# clocks sampled during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([c.strip() for c in line.split(",")])
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.t.join(timeout=2)
+        sm = [float(r[1]) for r in self.rows if len(r) >= 9 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) >= 9 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows if len(r) >= 9 for i in range(4)
+                          if r[5 + i].lower() in ("active", "1")})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# CPU legs (oracle port: numpy FP64 restatement of the reference)
+# ---------------------------------------------------------------------------
+def _oracle_scene_run(args):
+    s, steps = args
+    from oracle import mpm_oracle as O
+    sp = s["dx"] / 2
+    sc = O.Scene(shape=s["shape"], dx=s["dx"], dt=s["dt"], damping=s["damping"], pmass=s["density"] * sp ** 3,
+                 vol0=sp ** 3, wall=s["wall"])
+    m = O.Model.elastic(s["model"], s["E"], s["nu"])
+    gr = O.Growth(A=s["growth_A"])
+    t0 = time.perf_counter()
+    st, caches = O.rollout(O.State.rest(s["x"]), m, sc, steps, advect=True, growth=gr)
+    n = s["x"].shape[0]
+    z3, z33 = np.zeros((n, 3)), np.zeros((n, 3, 3))
+    O.rollout_vjp(caches, z3, z3, z33, O.seed_detF(st.F), z33, advect=True, growth=gr)
+    return n * steps, time.perf_counter() - t0
+
+
+def cpu_sample(scenes, seconds, steps=2):
+    """Scenes of the workload (smallest first) until ~`seconds` of work."""
+    order = sorted(range(len(scenes)), key=lambda i: scenes[i]["x"].shape[0])
+    budget_units = None
+    picked = []
+    # calibrate on the smallest scene
+    units, dt = _oracle_scene_run((scenes[order[0]], steps))
+    rate = units / dt
+    budget_units = rate * seconds
+    acc = 0
+    for i in order[1:]:
+        u = scenes[i]["x"].shape[0] * steps
+        if acc + u > budget_units:
+            break
+        picked.append(i)
+        acc += u
+    return picked, steps
+
+
+def cpu_baseline(scenes, seconds):
+    picked, steps = cpu_sample(scenes, seconds)
+    tot_u, tot_t = 0, 0.0
+    for i in picked:
+        u, t = _oracle_scene_run((scenes[i], steps))
+        tot_u += u
+        tot_t += t
+    return {"value": tot_u / max(tot_t, 1e-9), "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"{len(picked)} smallest scenes of the workload ({tot_u} particle-steps), {steps} steps "
+                      f"fwd+adj each, numpy FP64 oracle, 1 thread"}
+
+
+def run_reference(a):
+    """--impl reference: the oracle port on all host cores (process pool over scenes)."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from morphompm_b200 import scenes as S
+    for k in ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS", "MKL_NUM_THREADS"):
+        os.environ[k] = "1"
+    scn = S.config4(n_scenes=a.scenes)
+    cores = os.cpu_count() or 1
+    import multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    steps = 2
+    picked, _ = cpu_sample(scn, 4.0, steps)        # per-core budget ~4 s of work per bench step
+    jobs = [(scn[i], steps) for i in picked[:max(cores * 2, 1)]]
+    vals = []
+    with ctx.Pool(cores) as pool:
+        for it in range(a.warmup + a.steps):
+            t0 = time.perf_counter()
+            res = pool.map(_oracle_scene_run, jobs)
+            dt = time.perf_counter() - t0
+            if it >= a.warmup:
+                vals.append(sum(u for u, _ in res) / dt)
+    v = float(np.median(vals))
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": a.gpus, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "scenes": a.scenes, "mpm_steps": a.mpm_steps},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
+                             "sample": f"{len(jobs)} scenes x {steps} steps fwd+adj per bench step, numpy FP64 "
+                                       f"oracle, {cores} processes"},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# algorithmic bytes per particle, per kernel kind (w = bytes per word)
+# ---------------------------------------------------------------------------
+def kernel_bytes_per_particle(kind, w):
+    """Unique bytes a kernel must move per particle (state and cotangent
+    fields it reads and writes, its payload record, 4-byte sort indices);
+    node records are added separately."""
+    table = {
+        "prepass": 24 * w + 16 * w + 4 + 4,        # x v C F (+ growth law) -> payload, perm, scene id
+        "p2g": 16 * w,                             # payload record once
+        "g2p": 12 * w + 24 * w + 4 + 4 + 4,        # x F -> x v C F, perm, key, scene id
+        "bwd_payload": 36 * w + 16 * w + 4 + 4,
+        "bwd_p2g": 16 * w,
+        "bwd_particle": (24 + 9 + 24 + 24) * w + 8 + 4 + 4 + 4,
+    }
+    return table.get(kind)
+
+
+def node_bytes(kind, w):
+    return {"p2g": 4 * w, "bwd_p2g": 8 * w, "g2p": 4 * w, "bwd_particle": 8 * w}.get(kind, 0)
+
+
+# ---------------------------------------------------------------------------
+def main():
+    a = parse()
+    if a.impl == "reference":
+        return run_reference(a)
+    import torch
+    import torch.distributed as dist
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        torch.cuda.set_device(local)
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    dev = torch.device("cuda", torch.cuda.current_device())
+    from morphompm_b200 import scenes as S
+    from morphompm_b200.batch import Batch, host_slab, load_tuned
+    from morphompm_b200.trajectory import sqrt_schedule
+
+    scn = S.config4(seed=4 + 1000 * rank, n_scenes=a.scenes)
+    n_tot = sum(s["x"].shape[0] for s in scn)
+    k = a.ckpt_every or sqrt_schedule(a.mpm_steps)
+    tuning = load_tuned(scn, torch.float32) or {}
+    b = Batch(scn, a.mpm_steps, dtype=torch.float32, ckpt_every=k, tuning=tuning)
+    slab_h = torch.from_numpy(host_slab(scn, np.float32)).pin_memory()
+    b.load(slab_h, non_blocking=False)
+    plan = b.plan
+
+    # capture once with every kernel bracketed to find the dominant kernel
+    from morphompm_b200 import _lib as L
+    counts = {}
+
+    def start_all():
+        counts["n0"] = plan.launch_count()
+        plan.profile_begin(L.KERNELS, max_launches=20000)
+    b.capture(pre_capture=start_all)
+    launches_per_traj = plan.launch_count() - counts["n0"]
+    b.replay()
+    prof_all = plan.profile_end()
+    dominant = max(prof_all, key=lambda kk: prof_all[kk][0])
+
+    # re-capture with only the dominant kernel bracketed; this graph is timed
+    b.graph = None
+    b.capture(pre_capture=lambda: plan.profile_begin([dominant], max_launches=20000))
+    for _ in range(a.warmup):
+        b.replay()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clocks = ClockSampler(dev.index if dev.index is not None else 0)
+    clocks.start()
+    s = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(s)
+    for _ in range(a.steps):
+        b.replay()
+    e1.record(s)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    clk = clocks.stop()
+    prof = plan.profile_end()
+    if world > 1:
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    ms_per = ms / a.steps
+    units = n_tot * a.mpm_steps * world
+    value = units / (ms_per / 1e3)
+
+    # end to end through the public API: pinned host slab -> device, trajectory,
+    # per-scene loss and dL/dg back to the host
+    loss_h = torch.empty(len(scn), dtype=torch.float64).pin_memory()
+    grad_h = torch.empty(len(scn), dtype=torch.float64).pin_memory()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    e0.record(s)
+    for _ in range(a.steps):
+        b.load(slab_h, non_blocking=True)
+        b.replay()
+        loss_h.copy_(b.loss, non_blocking=True)
+        grad_h.copy_(b.dloss_dg, non_blocking=True)
+    e1.record(s)
+    torch.cuda.synchronize()
+    ms_e2e = e0.elapsed_time(e1)
+    if world > 1:
+        t = torch.tensor([ms_e2e], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_e2e = float(t.item())
+    e2e = {"value": units / (ms_e2e / a.steps / 1e3), "unit": UNIT,
+           "h2d_bytes_per_step": int(slab_h.numel() * slab_h.element_size()),
+           "d2h_bytes_per_step": int(2 * 8 * len(scn))}
+
+    # roofline of the dominant kernel (HBM bound: no dense contraction here)
+    tot_ms, nl = prof.get(dominant, (float("nan"), 0))
+    avg_ms = tot_ms / max(nl, 1)
+    w = 4
+    nodes_per_launch = None
+    bpp = kernel_bytes_per_particle(dominant, w)
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        peak, peak_src = float(peaks["hbm_gbs"]), "measured"
+    except Exception:
+        peak, peak_src = 6650.0, "fallback"
+    achieved = None
+    if bpp is not None and nl:
+        alg = bpp * n_tot + node_bytes(dominant, w) * 0.2 * n_tot
+        achieved = alg / (avg_ms / 1e3) / 1e9
+    roof = {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak, "peak_source": peak_src,
+            "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
+            "traffic": None, "avg_launch_ms": avg_ms, "launches": nl}
+    # whole step against the algorithmic bytes per particle-step fwd+adj
+    # (w*(156 + 32*G_touched/n), G_touched/n ~ 0.2 at 8 particles per cell)
+    step_bytes = w * (156 + 32 * 0.2) * n_tot * a.mpm_steps
+    step_roof = {"bytes_per_particle_step": w * (156 + 32 * 0.2), "achieved_gbs": step_bytes / (ms_per / 1e3) / 1e9,
+                 "frac": step_bytes / (ms_per / 1e3) / 1e9 / peak}
+    fallbacks = plan.fp64_fallbacks()
+
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
+            "ms_per_step": ms_per, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "scenes": len(scn), "particles": n_tot * world,
+                       "mpm_steps": a.mpm_steps, "ckpt_every": k, "l2": "inputs larger than L2 "
+                       f"({n_tot * 24 * 4 / 1e6:.0f} MB state per GPU)", "schedule": plan.tuning or "defaults",
+                       "parallelism": f"{world} independent batches (no collective)"},
+            "roofline": roof, "step_roofline": step_roof, "e2e": e2e,
+            "gpu_launches": int(launches_per_traj * a.steps), "clocks": clk,
+            "kernel_ms_per_trajectory": {kk: round(v[0], 3) for kk, v in prof_all.items()},
+            "fp64_hencky_fallbacks_per_trajectory": None}
+    line["fp64_hencky_fallbacks_per_trajectory"] = fallbacks / max(1, a.warmup + a.steps + 3)
+
+    if rank == 0 and not a.no_plain:
+        line["fp64_plain"] = plain_leg(scn, a, value)
+    if rank == 0 and not a.no_cpu:
+        line["cpu_baseline"] = cpu_baseline(scn, a.cpu_seconds)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        b.graph = None
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def plain_leg(scn, a, value32):
+    """FP64 plain path: one scene at a time, eager launches per step (the
+    drop-in transfer path), same trajectory.  Timed on a sample of scenes
+    spread over the size range; FP32 error vs FP64 on the same scenes."""
+    import torch
+    from morphompm_b200.batch import Batch, host_slab
+    idx = sorted(range(len(scn)), key=lambda i: scn[i]["x"].shape[0])
+    sample = [idx[int(round(q * (len(idx) - 1)))] for q in np.linspace(0.0, 1.0, 6)]
+    units, secs = 0, 0.0
+    errs = {"F": 0.0, "x": 0.0, "dLdg_rel": 0.0}
+    for i in sample:
+        s = scn[i]
+        b64 = Batch([s], a.mpm_steps, dtype=torch.float64, ckpt_every=a.ckpt_every or None)
+        b64.load(host_slab([s], np.float64), non_blocking=False)
+        b64.run()                                     # warm-up
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        b64.run()
+        torch.cuda.synchronize()
+        secs += time.perf_counter() - t0
+        units += s["x"].shape[0] * a.mpm_steps
+        b32 = Batch([s], a.mpm_steps, dtype=torch.float32, ckpt_every=a.ckpt_every or None)
+        b32.load(host_slab([s], np.float32), non_blocking=False)
+        b32.run()
+        torch.cuda.synchronize()
+        f64 = b64.rollout.final.cpu().numpy()
+        f32 = b32.rollout.final.double().cpu().numpy()
+        errs["F"] = max(errs["F"], float(np.max(np.abs(f64[15:24] - f32[15:24]))))
+        errs["x"] = max(errs["x"], float(np.max(np.abs(f64[0:3] - f32[0:3]))))
+        g64, g32 = float(b64.dloss_dg[0]), float(b32.dloss_dg[0])
+        errs["dLdg_rel"] = max(errs["dLdg_rel"], abs(g64 - g32) / max(abs(g64), 1e-300))
+    v64 = units / secs
+    return {"value": v64, "unit": UNIT, "sample": f"{len(sample)} scenes spread over the size range, "
+            f"{a.mpm_steps} steps fwd+adj each, eager launches, FP64", "fp32_batched_over_fp64_plain": value32 / v64,
+            "fp32_error_vs_fp64": errs}
+
+
+if __name__ == "__main__":
+    main()

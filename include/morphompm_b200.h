@@ -36,6 +36,20 @@ extern "C" {
 #define MPM_MODEL_HENCKY            1   /* constitutive.py:42-75  */
 #define MPM_MODEL_HERSCHEL_BULKLEY  2   /* constitutive.py:106-147 */
 
+/* ---- kernel kinds (for mpm_plan_profile_begin) ---- */
+#define MPM_K_BIN           0   /* cell keys                                 */
+#define MPM_K_SORT          1   /* radix-sort passes (4 kernels per pass)    */
+#define MPM_K_MARK          2   /* cell ranges + tile flags                  */
+#define MPM_K_COMPACT       3   /* active-tile list                          */
+#define MPM_K_PREPASS       4   /* stress + P2G payload                      */
+#define MPM_K_P2G           5   /* P2G scatter + grid update                 */
+#define MPM_K_G2P           6   /* G2P + advection + F update                */
+#define MPM_K_BWD_PAYLOAD   7   /* G2P-adjoint payload                       */
+#define MPM_K_BWD_P2G       8   /* gv_b scatter + grid adjoint               */
+#define MPM_K_BWD_PARTICLE  9   /* P2G adjoint + constitutive VJP            */
+#define MPM_K_REDUCE       10   /* per-scene reductions                      */
+#define MPM_K_COUNT        11
+
 /* ---- arithmetic types ---- */
 #define MPM_F32 4
 #define MPM_F64 8
@@ -105,6 +119,19 @@ int mpm_plan_bind(MpmPlan* plan, void* workspace, void* stream);
 int mpm_plan_read_status(MpmPlan* plan, int32_t* status, void* stream);
 /* Number of FP32 Hencky evaluations that took the FP64 path since bind. */
 int mpm_plan_read_fp64_fallbacks(MpmPlan* plan, int64_t* count, void* stream);
+
+/* Bracket every launch of the kernel kinds in kind_mask (bit k = MPM_K_k) with
+ * CUDA events, recorded as external event nodes when the stream is being
+ * captured, so graph replays re-record them.  At most max_launches launches
+ * are bracketed.  mpm_plan_profile_end synchronises and writes, per kind, the
+ * summed device time (ms) and the number of bracketed launches (arrays of
+ * MPM_K_COUNT entries); for a captured graph the times are those of its last
+ * replay. */
+int mpm_plan_profile_begin(MpmPlan* plan, uint32_t kind_mask, int32_t max_launches);
+int mpm_plan_profile_end(MpmPlan* plan, double* ms_per_kind, int32_t* launches_per_kind);
+/* Kernel launches issued by this plan so far (host-side count; a captured
+ * graph's launches are counted once, at capture). */
+int64_t mpm_plan_launch_count(const MpmPlan* plan);
 
 /* Optional per-particle growth field phi_p (growth_mode 1), real type. */
 int mpm_plan_set_growth_field(MpmPlan* plan, const void* phi);

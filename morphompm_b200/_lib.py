@@ -19,6 +19,9 @@ MPM_WARN_OUTSIDE = 8
 MPM_ERR_TAPE = 16
 MPM_ERR_UNSUPPORTED = 32
 
+KERNELS = ["bin", "sort", "mark", "compact", "prepass", "p2g", "g2p", "bwd_payload", "bwd_p2g",
+           "bwd_particle", "reduce"]
+
 MODEL_NEOHOOKEAN = 0
 MODEL_HENCKY = 1
 MODEL_HERSCHEL_BULKLEY = 2
@@ -65,6 +68,9 @@ EXPORTS = {
     "mpm_plan_read_status": (i32, [vp, C.POINTER(i32), vp]),
     "mpm_plan_read_fp64_fallbacks": (i32, [vp, C.POINTER(i64), vp]),
     "mpm_plan_set_growth_field": (i32, [vp, vp]),
+    "mpm_plan_profile_begin": (i32, [vp, C.c_uint32, i32]),
+    "mpm_plan_profile_end": (i32, [vp, C.POINTER(f64), C.POINTER(i32)]),
+    "mpm_plan_launch_count": (i64, [vp]),
     "mpm_step_fwd": (i32, [vp, C.POINTER(MpmParticles), C.POINTER(MpmParticles), i32, i32, vp, vp]),
     "mpm_step_bwd": (i32, [vp, C.POINTER(MpmParticles), vp, C.POINTER(MpmCotangents),
                            C.POINTER(MpmCotangents), vp, i32, i32, vp, vp]),

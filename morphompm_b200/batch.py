@@ -99,8 +99,8 @@ class Batch:
     def run(self):
         return self.rollout.run(self.slab0)
 
-    def capture(self):
-        self.graph = self.rollout.capture(self.slab0)
+    def capture(self, pre_capture=None):
+        self.graph = self.rollout.capture(self.slab0, pre_capture)
         return self.graph
 
     def replay(self):

@@ -52,6 +52,12 @@ struct MpmPlan {
     char* ws = nullptr;
     const void* phi = nullptr;
     int n_sm = 148;
+    // profiling
+    uint32_t prof_mask = 0;
+    int prof_max = 0, prof_n = 0;
+    std::vector<cudaEvent_t> ev0, ev1;
+    std::vector<int> ev_kind;
+    long long launches = 0;
 };
 
 namespace {
@@ -91,6 +97,35 @@ Tape<R> make_tape(MpmPlan* P, char* t) {
     tp.grid = reinterpret_cast<R*>(t + P->t_grid);
     return tp;
 }
+
+void record_event(cudaEvent_t e, cudaStream_t st) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaStreamIsCapturing(st, &cs);
+    cudaEventRecordWithFlags(e, st, cs == cudaStreamCaptureStatusActive ? cudaEventRecordExternal
+                                                                        : cudaEventRecordDefault);
+}
+
+// Brackets one launch site: counts its kernels and, when profiling this kind,
+// records start/stop events around it.
+struct Site {
+    MpmPlan* P;
+    cudaStream_t st;
+    bool on;
+    Site(MpmPlan* p, int kind, int kernels, cudaStream_t s) : P(p), st(s) {
+        P->launches += kernels;
+        on = ((P->prof_mask >> kind) & 1u) && P->prof_n < P->prof_max;
+        if (on) {
+            P->ev_kind[P->prof_n] = kind;
+            record_event(P->ev0[P->prof_n], st);
+        }
+    }
+    ~Site() {
+        if (on) {
+            record_event(P->ev1[P->prof_n], st);
+            ++P->prof_n;
+        }
+    }
+};
 
 inline int grid_for(long long n, int block) { return (int)std::max<long long>(1, (n + block - 1) / block); }
 
@@ -155,6 +190,7 @@ int run_sort(MpmPlan* P, const unsigned* keys, unsigned* skeys, unsigned* perm, 
     const int nblk = P->nblk_sort;
     const unsigned* ksrc = keys;
     const unsigned* vsrc = nullptr;
+    Site site(P, MPM_K_SORT, 4 * P->passes, st);
     for (int pass = 0; pass < P->passes; ++pass) {
         const int shift = pass * RADIX_BITS;
         unsigned* kdst = (pass == P->passes - 1) ? skeys : kalt[pass & 1];
@@ -178,18 +214,24 @@ int step_fwd_T(MpmPlan* P, const MpmParticles& in, MpmParticles& out, int advect
     const int g = grid_for(P->n, B);
     unsigned* keys = at<unsigned>(P, P->o_keys);
     R* payload = at<R>(P, P->o_payload);
-    bin_kernel<R><<<g, B, 0, st>>>(ctx, in, keys);
+    { Site s(P, MPM_K_BIN, 1, st); bin_kernel<R><<<g, B, 0, st>>>(ctx, in, keys); }
     int rc = run_sort(P, keys, tp.skeys, tp.perm, st);
     if (rc) return rc;
-    mark_kernel<<<g, B, 0, st>>>(ctx, tp.skeys, 1);
-    compact_tiles_kernel<<<1, 1024, 0, st>>>(ctx.tile_flag, P->n_tiles, tp.tile_slot, tp.active, tp.n_active,
-                                             P->active_cap, ctx.status);
-    prepass_kernel<R><<<g, B, 0, st>>>(ctx, in, tp.perm, payload, t);
+    { Site s(P, MPM_K_MARK, 1, st); mark_kernel<<<g, B, 0, st>>>(ctx, tp.skeys, 1); }
+    {
+        Site s(P, MPM_K_COMPACT, 1, st);
+        compact_tiles_kernel<<<1, 1024, 0, st>>>(ctx.tile_flag, P->n_tiles, tp.tile_slot, tp.active, tp.n_active,
+                                                 P->active_cap, ctx.status);
+    }
+    { Site s(P, MPM_K_PREPASS, 1, st); prepass_kernel<R><<<g, B, 0, st>>>(ctx, in, tp.perm, payload, t); }
     rc = check_launch();
     if (rc) return rc;
-    rc = launch_scatter<R>(P, 0, ctx, payload, tp.active, tp.n_active, tp.grid, nullptr, advect, st);
+    {
+        Site s(P, MPM_K_P2G, 1, st);
+        rc = launch_scatter<R>(P, 0, ctx, payload, tp.active, tp.n_active, tp.grid, nullptr, advect, st);
+    }
     if (rc) return rc;
-    g2p_kernel<R, T><<<g, B, 0, st>>>(ctx, tp, in, out, advect);
+    { Site s(P, MPM_K_G2P, 1, st); g2p_kernel<R, T><<<g, B, 0, st>>>(ctx, tp, in, out, advect); }
     return check_launch();
 }
 
@@ -203,17 +245,28 @@ int step_bwd_T(MpmPlan* P, const MpmParticles& in, const void* outC, const MpmCo
     R* payload = at<R>(P, P->o_payload);
     R* gridb = at<R>(P, P->o_gridb);
     double* dbuf = at<double>(P, P->o_dbuf);
-    mark_kernel<<<g, B, 0, st>>>(ctx, tp.skeys, 0);
-    bwd_payload_kernel<R><<<g, B, 0, st>>>(ctx, tp.perm, in, ob, payload, advect);
+    { Site s(P, MPM_K_MARK, 1, st); mark_kernel<<<g, B, 0, st>>>(ctx, tp.skeys, 0); }
+    {
+        Site s(P, MPM_K_BWD_PAYLOAD, 1, st);
+        bwd_payload_kernel<R><<<g, B, 0, st>>>(ctx, tp.perm, in, ob, payload, advect);
+    }
     int rc = check_launch();
     if (rc) return rc;
-    rc = launch_scatter<R>(P, 1, ctx, payload, tp.active, tp.n_active, gridb, tp.grid, advect, st);
+    {
+        Site s(P, MPM_K_BWD_P2G, 1, st);
+        rc = launch_scatter<R>(P, 1, ctx, payload, tp.active, tp.n_active, gridb, tp.grid, advect, st);
+    }
     if (rc) return rc;
     bool want_dA = growth_grad != nullptr && P->any_growth;
-    bwd_particle_kernel<R, T><<<g, B, 0, st>>>(ctx, tp, gridb, in, static_cast<const R*>(outC), ob, ib,
-                                               want_dA ? dbuf : nullptr, advect, t);
-    if (want_dA)
+    {
+        Site s(P, MPM_K_BWD_PARTICLE, 1, st);
+        bwd_particle_kernel<R, T><<<g, B, 0, st>>>(ctx, tp, gridb, in, static_cast<const R*>(outC), ob, ib,
+                                                   want_dA ? dbuf : nullptr, advect, t);
+    }
+    if (want_dA) {
+        Site s(P, MPM_K_REDUCE, 1, st);
         scene_reduce_kernel<<<(int)P->scenes.size(), 256, 0, st>>>(ctx, dbuf, growth_grad, 1, 0);
+    }
     return check_launch();
 }
 
@@ -334,7 +387,49 @@ int mpm_plan_create(const MpmScene* scenes, int32_t n_scenes, int32_t real_bytes
     return MPM_OK;
 }
 
-void mpm_plan_destroy(MpmPlan* plan) { delete plan; }
+void mpm_plan_destroy(MpmPlan* plan) {
+    if (!plan) return;
+    for (cudaEvent_t e : plan->ev0) cudaEventDestroy(e);
+    for (cudaEvent_t e : plan->ev1) cudaEventDestroy(e);
+    delete plan;
+}
+
+int mpm_plan_profile_begin(MpmPlan* P, uint32_t kind_mask, int32_t max_launches) {
+    if (!P || max_launches < 1 || (kind_mask >> MPM_K_COUNT) != 0) return MPM_ERR_ARG;
+    while ((int)P->ev0.size() < max_launches) {
+        cudaEvent_t a, b;
+        if (cudaEventCreate(&a) != cudaSuccess || cudaEventCreate(&b) != cudaSuccess) return MPM_ERR_CUDA;
+        P->ev0.push_back(a);
+        P->ev1.push_back(b);
+    }
+    P->ev_kind.assign(P->ev0.size(), -1);
+    P->prof_mask = kind_mask;
+    P->prof_max = max_launches;
+    P->prof_n = 0;
+    return MPM_OK;
+}
+
+int mpm_plan_profile_end(MpmPlan* P, double* ms_per_kind, int32_t* launches_per_kind) {
+    if (!P || !ms_per_kind || !launches_per_kind) return MPM_ERR_ARG;
+    for (int k = 0; k < MPM_K_COUNT; ++k) {
+        ms_per_kind[k] = 0.0;
+        launches_per_kind[k] = 0;
+    }
+    for (int i = 0; i < P->prof_n; ++i) {
+        if (cudaEventSynchronize(P->ev1[i]) != cudaSuccess) return MPM_ERR_CUDA;
+        float ms = 0.f;
+        if (cudaEventElapsedTime(&ms, P->ev0[i], P->ev1[i]) != cudaSuccess) return MPM_ERR_CUDA;
+        int k = P->ev_kind[i];
+        if (k >= 0 && k < MPM_K_COUNT) {
+            ms_per_kind[k] += ms;
+            launches_per_kind[k] += 1;
+        }
+    }
+    P->prof_mask = 0;
+    return MPM_OK;
+}
+
+int64_t mpm_plan_launch_count(const MpmPlan* P) { return P ? P->launches : -1; }
 
 int mpm_plan_workspace_bytes(const MpmPlan* P, size_t* bytes) {
     if (!P || !bytes) return MPM_ERR_ARG;
@@ -481,6 +576,7 @@ int mpm_loss_detF(MpmPlan* P, const void* F, int64_t sp9, int64_t sc9, double* l
     Ctx ctx = make_ctx(P);
     double* dbuf = at<double>(P, P->o_dbuf);
     int g = grid_for(P->n, 256);
+    Site site(P, MPM_K_REDUCE, 2, st);
     if (P->real_bytes == 4)
         loss_detF_kernel<float><<<g, 256, 0, st>>>(ctx, (const float*)F, sp9, sc9, dbuf, (float*)F_bar);
     else
@@ -496,6 +592,7 @@ int mpm_loss_mse(MpmPlan* P, const void* x, int64_t sp3, int64_t sc3, const void
     Ctx ctx = make_ctx(P);
     double* dbuf = at<double>(P, P->o_dbuf);
     int g = grid_for(P->n, 256);
+    Site site(P, MPM_K_REDUCE, 2, st);
     if (P->real_bytes == 4)
         loss_mse_kernel<float><<<g, 256, 0, st>>>(ctx, (const float*)x, sp3, sc3, (const float*)x_obs, dbuf,
                                                   (float*)x_bar);

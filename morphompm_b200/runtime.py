@@ -170,6 +170,24 @@ class Plan:
                 "fallbacks")
         return v.value
 
+    # -- profiling ---------------------------------------------------------------
+    def profile_begin(self, kinds, max_launches: int = 1 << 16):
+        """Bracket the launches of the named kernel kinds with CUDA events."""
+        mask = 0
+        for k in kinds:
+            mask |= 1 << L.KERNELS.index(k)
+        L.check(self.lib.mpm_plan_profile_begin(self.handle, mask, int(max_launches)), "profile_begin")
+
+    def profile_end(self) -> dict:
+        """{kind: (total_ms, launches)} of the bracketed launches."""
+        ms = (C.c_double * len(L.KERNELS))()
+        cnt = (C.c_int32 * len(L.KERNELS))()
+        L.check(self.lib.mpm_plan_profile_end(self.handle, ms, cnt), "profile_end")
+        return {k: (ms[i], cnt[i]) for i, k in enumerate(L.KERNELS) if cnt[i] > 0}
+
+    def launch_count(self) -> int:
+        return int(self.lib.mpm_plan_launch_count(self.handle))
+
     # -- steps ---------------------------------------------------------------
     def step_fwd(self, pin: L.MpmParticles, pout: L.MpmParticles, advect: bool, t: int,
                  tape: Optional["TapeBuf"] = None, stream=None):

@@ -155,15 +155,19 @@ class Rollout:
         self.seed(stream)
         return self.backward(None, stream)
 
-    def capture(self, slab0: torch.Tensor):
+    def capture(self, slab0: torch.Tensor, pre_capture=None):
         """Capture forward + loss + adjoint from the fixed input slab0 into one
-        CUDA graph (replay with ``replay()``)."""
+        CUDA graph (replay with ``replay()``).  ``pre_capture`` runs after the
+        eager warm-up, just before capture begins."""
         self._graph_in = slab0
         s = torch.cuda.Stream(device=self.plan.device)
         s.wait_stream(torch.cuda.current_stream())
         with torch.cuda.stream(s):
             self.run(slab0)          # warm-up outside the graph (loads, attributes)
         torch.cuda.current_stream().wait_stream(s)
+        torch.cuda.synchronize()
+        if pre_capture is not None:
+            pre_capture()
         g = torch.cuda.CUDAGraph()
         with torch.cuda.graph(g):
             self.run(slab0)

@@ -44,8 +44,10 @@ struct MpmPlan {
     int TN = 0, active_cap = 0;
     bool any_growth = false;
     // workspace offsets
-    size_t o_scenes, o_aux, o_scene_of, o_tile_scene, o_status, o_cell_first, o_cell_last, o_tile_flag;
-    size_t o_keys, o_kalt0, o_valt0, o_kalt1, o_valt1, o_hist, o_totals, o_payload, o_gridb, o_dbuf, o_tape;
+    size_t o_scenes, o_aux, o_scene_of, o_tile_scene, o_status, o_cell_seg, o_seg_first, o_seg_last, o_blk;
+    size_t o_tile_flag, o_keys, o_kalt0, o_valt0, o_kalt1, o_valt1, o_hist, o_totals, o_payload, o_sums, o_gridb;
+    size_t o_dbuf, o_tape;
+    int nblk_seg = 1;
     size_t ws_bytes = 0;
     // tape offsets
     size_t t_skeys, t_perm, t_slot, t_active, t_nact, t_grid, tape_bytes = 0;
@@ -73,8 +75,11 @@ Ctx make_ctx(MpmPlan* P) {
     c.tile_scene = at<const int>(P, P->o_tile_scene);
     c.status = at<int>(P, P->o_status);
     c.fallbacks = reinterpret_cast<unsigned long long*>(P->ws + P->o_status + 64);
-    c.cell_first = at<int>(P, P->o_cell_first);
-    c.cell_last = at<int>(P, P->o_cell_last);
+    c.cell_seg = at<int>(P, P->o_cell_seg);
+    c.seg_first = at<int>(P, P->o_seg_first);
+    c.seg_last = at<int>(P, P->o_seg_last);
+    c.n_seg = reinterpret_cast<int*>(P->ws + P->o_status + 32);
+    c.blk_count = at<unsigned>(P, P->o_blk);
     c.tile_flag = at<int>(P, P->o_tile_flag);
     c.phi = P->phi;
     c.n = P->n;
@@ -134,51 +139,49 @@ inline int check_launch() {
     return e == cudaSuccess ? MPM_OK : MPM_ERR_CUDA;
 }
 
-template <typename R, int T, int MODE>
-void* scatter_fn(int oxb) {
-    if constexpr (sizeof(R) == 4) {
-        if (oxb == 3) return (void*)scatter_kernel<R, T, MODE, 3>;
-    }
-    return (void*)scatter_kernel<R, T, MODE, 1>;
+// segment table of the sorted keys (and, in the forward, the active tile flags)
+int build_segments(MpmPlan* P, const Ctx& ctx, const unsigned* skeys, int flag_tiles, cudaStream_t st) {
+    Site site(P, MPM_K_MARK, 3, st);
+    seg_count_kernel<<<P->nblk_seg, SEG_THREADS, 0, st>>>(ctx, skeys, flag_tiles);
+    seg_scan_kernel<<<1, 1024, 0, st>>>(ctx, P->nblk_seg);
+    seg_write_kernel<<<P->nblk_seg, SEG_THREADS, 0, st>>>(ctx, skeys);
+    return check_launch();
 }
 
 template <typename R, int MODE>
-void* scatter_dispatch(int T, int oxb) {
-    if (T == 4) return scatter_fn<R, 4, MODE>(oxb);
-    if (T == 16) return scatter_fn<R, 16, MODE>(oxb);
-    return scatter_fn<R, 8, MODE>(oxb);
+void* sums_fn(int oxb) {
+    if constexpr (sizeof(R) == 4) {
+        if (oxb == 3) return (void*)cell_sums_kernel<R, MODE, 3>;
+    }
+    return (void*)cell_sums_kernel<R, MODE, 1>;
 }
 
-template <typename R>
-size_t scatter_smem(int T, int mode) { return (size_t)T * T * TILE_Z * (mode == 0 ? 4 : 3) * sizeof(R); }
+template <typename R, int MODE>
+void* nodes_fn(int T) {
+    if (T == 4) return (void*)node_sums_kernel<R, 4, MODE>;
+    if (T == 16) return (void*)node_sums_kernel<R, 16, MODE>;
+    return (void*)node_sums_kernel<R, 8, MODE>;
+}
 
+// two-phase P2G: per-cell stencil sums, then per-node gather + grid epilogue
 template <typename R>
-int launch_scatter(MpmPlan* P, int mode, const Ctx& ctx, const R* payload, const int* active, const int* nact,
-                   R* grid_out, const R* grid_fwd, int advect, cudaStream_t st) {
-    const int T = P->tune.tile_xy;
-    int oxb = P->tune.scatter_oxb;
-    void* fn = mode == 0 ? scatter_dispatch<R, 0>(T, oxb) : scatter_dispatch<R, 1>(T, oxb);
-    size_t smem = scatter_smem<R>(T, mode);
+int launch_p2g(MpmPlan* P, int mode, const Ctx& ctx, const R* payload, const int* active, const int* nact,
+               R* grid_out, const R* grid_fwd, int advect, cudaStream_t st) {
+    R* S = at<R>(P, P->o_sums);
+    long long cap = P->n;
+    int blocks1 = (int)std::min<long long>((P->n + 127) / 128, (long long)P->n_sm * 16);
+    blocks1 = std::max(1, blocks1);
+    void* f1 = mode == 0 ? sums_fn<R, 0>(P->tune.scatter_oxb) : sums_fn<R, 1>(P->tune.scatter_oxb);
+    void* a1[] = {(void*)&ctx, (void*)&payload, (void*)&S, (void*)&cap};
+    if (cudaLaunchKernel(f1, dim3(blocks1), dim3(128), a1, 0, st) != cudaSuccess) return MPM_ERR_CUDA;
+    const R* Sc = S;
     int ctas = P->n_sm * std::max(1, P->tune.scatter_ctas_per_sm);
     ctas = std::max(1, std::min(ctas, P->active_cap));
-    void* args[] = {(void*)&ctx, (void*)&payload, (void*)&active, (void*)&nact, (void*)&grid_out,
-                    (void*)&grid_fwd, (void*)&advect};
-    cudaError_t e = cudaLaunchKernel(fn, dim3(ctas), dim3(256), args, smem, st);
-    return e == cudaSuccess ? MPM_OK : MPM_ERR_CUDA;
-}
-
-template <typename R>
-int set_smem_attrs(MpmPlan* P) {
-    const int T = P->tune.tile_xy;
-    for (int mode = 0; mode < 2; ++mode) {
-        for (int oxb : {1, 3}) {
-            void* fn = mode == 0 ? scatter_dispatch<R, 0>(T, oxb) : scatter_dispatch<R, 1>(T, oxb);
-            size_t smem = scatter_smem<R>(T, mode);
-            if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
-                return MPM_ERR_CUDA;
-        }
-    }
-    return MPM_OK;
+    void* f2 = mode == 0 ? nodes_fn<R, 0>(P->tune.tile_xy) : nodes_fn<R, 1>(P->tune.tile_xy);
+    void* a2[] = {(void*)&ctx, (void*)&Sc, (void*)&cap, (void*)&active, (void*)&nact, (void*)&grid_out,
+                  (void*)&grid_fwd, (void*)&advect};
+    P->launches += 1;   // the Site around this call counts one
+    return cudaLaunchKernel(f2, dim3(ctas), dim3(256), a2, 0, st) == cudaSuccess ? MPM_OK : MPM_ERR_CUDA;
 }
 
 // stable LSD radix sort of the binning keys -> tape (skeys, perm)
@@ -217,7 +220,8 @@ int step_fwd_T(MpmPlan* P, const MpmParticles& in, MpmParticles& out, int advect
     { Site s(P, MPM_K_BIN, 1, st); bin_kernel<R><<<g, B, 0, st>>>(ctx, in, keys); }
     int rc = run_sort(P, keys, tp.skeys, tp.perm, st);
     if (rc) return rc;
-    { Site s(P, MPM_K_MARK, 1, st); mark_kernel<<<g, B, 0, st>>>(ctx, tp.skeys, 1); }
+    rc = build_segments(P, ctx, tp.skeys, 1, st);
+    if (rc) return rc;
     {
         Site s(P, MPM_K_COMPACT, 1, st);
         compact_tiles_kernel<<<1, 1024, 0, st>>>(ctx.tile_flag, P->n_tiles, tp.tile_slot, tp.active, tp.n_active,
@@ -228,7 +232,7 @@ int step_fwd_T(MpmPlan* P, const MpmParticles& in, MpmParticles& out, int advect
     if (rc) return rc;
     {
         Site s(P, MPM_K_P2G, 1, st);
-        rc = launch_scatter<R>(P, 0, ctx, payload, tp.active, tp.n_active, tp.grid, nullptr, advect, st);
+        rc = launch_p2g<R>(P, 0, ctx, payload, tp.active, tp.n_active, tp.grid, nullptr, advect, st);
     }
     if (rc) return rc;
     { Site s(P, MPM_K_G2P, 1, st); g2p_kernel<R, T><<<g, B, 0, st>>>(ctx, tp, in, out, advect); }
@@ -245,16 +249,17 @@ int step_bwd_T(MpmPlan* P, const MpmParticles& in, const void* outC, const MpmCo
     R* payload = at<R>(P, P->o_payload);
     R* gridb = at<R>(P, P->o_gridb);
     double* dbuf = at<double>(P, P->o_dbuf);
-    { Site s(P, MPM_K_MARK, 1, st); mark_kernel<<<g, B, 0, st>>>(ctx, tp.skeys, 0); }
+    int rc = build_segments(P, ctx, tp.skeys, 0, st);
+    if (rc) return rc;
     {
         Site s(P, MPM_K_BWD_PAYLOAD, 1, st);
         bwd_payload_kernel<R><<<g, B, 0, st>>>(ctx, tp.perm, in, ob, payload, advect);
     }
-    int rc = check_launch();
+    rc = check_launch();
     if (rc) return rc;
     {
         Site s(P, MPM_K_BWD_P2G, 1, st);
-        rc = launch_scatter<R>(P, 1, ctx, payload, tp.active, tp.n_active, gridb, tp.grid, advect, st);
+        rc = launch_p2g<R>(P, 1, ctx, payload, tp.active, tp.n_active, gridb, tp.grid, advect, st);
     }
     if (rc) return rc;
     bool want_dA = growth_grad != nullptr && P->any_growth;
@@ -368,8 +373,11 @@ int mpm_plan_create(const MpmScene* scenes, int32_t n_scenes, int32_t real_bytes
     P->o_scene_of = L.take(n * 4);
     P->o_tile_scene = L.take(nt * 4);
     P->o_status = L.take(128);
-    P->o_cell_first = L.take((size_t)P->n_keys * 4);
-    P->o_cell_last = L.take((size_t)P->n_keys * 4);
+    P->nblk_seg = (int)((P->n + SEG_TILE - 1) / SEG_TILE);
+    P->o_cell_seg = L.take((size_t)P->n_keys * 4);
+    P->o_seg_first = L.take(n * 4);
+    P->o_seg_last = L.take(n * 4);
+    P->o_blk = L.take((size_t)P->nblk_seg * 4);
     P->o_tile_flag = L.take(nt * 4);
     P->o_keys = L.take(n * 4);
     P->o_kalt0 = L.take(n * 4);
@@ -379,6 +387,7 @@ int mpm_plan_create(const MpmScene* scenes, int32_t n_scenes, int32_t real_bytes
     P->o_hist = L.take((size_t)RADIX * P->nblk_sort * 4);
     P->o_totals = L.take(RADIX * 4);
     P->o_payload = L.take(n * PAYLOAD * R);
+    P->o_sums = L.take(27 * n * 4 * R);
     P->o_gridb = L.take((size_t)P->active_cap * P->TN * 4 * R);
     P->o_dbuf = L.take(n * 8);
     P->o_tape = L.take(P->tape_bytes);
@@ -450,8 +459,6 @@ int mpm_plan_bind(MpmPlan* P, void* workspace, void* stream) {
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return MPM_ERR_CUDA;
     cudaDeviceGetAttribute(&P->n_sm, cudaDevAttrMultiProcessorCount, dev);
-    int rc = P->real_bytes == 4 ? set_smem_attrs<float>(P) : set_smem_attrs<double>(P);
-    if (rc) return rc;
     if (cudaMemcpyAsync(P->ws + P->o_scenes, P->scenes.data(), sizeof(MpmScene) * P->scenes.size(),
                         cudaMemcpyHostToDevice, st) != cudaSuccess ||
         cudaMemcpyAsync(P->ws + P->o_aux, P->aux.data(), sizeof(SceneAux) * P->aux.size(),
@@ -461,8 +468,7 @@ int mpm_plan_bind(MpmPlan* P, void* workspace, void* stream) {
         cudaMemcpyAsync(P->ws + P->o_tile_scene, P->tile_scene.data(), 4 * P->tile_scene.size(),
                         cudaMemcpyHostToDevice, st) != cudaSuccess ||
         cudaMemsetAsync(P->ws + P->o_status, 0, 128, st) != cudaSuccess ||
-        cudaMemsetAsync(P->ws + P->o_cell_first, 0, (size_t)P->n_keys * 4, st) != cudaSuccess ||
-        cudaMemsetAsync(P->ws + P->o_cell_last, 0, (size_t)P->n_keys * 4, st) != cudaSuccess ||
+        cudaMemsetAsync(P->ws + P->o_cell_seg, 0, (size_t)P->n_keys * 4, st) != cudaSuccess ||
         cudaMemsetAsync(P->ws + P->o_tile_flag, 0, (size_t)P->n_tiles * 4, st) != cudaSuccess)
         return MPM_ERR_CUDA;
     // the host tables are read by the copies above: wait before returning

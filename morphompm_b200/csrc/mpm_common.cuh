@@ -12,10 +12,8 @@
 
 namespace mpm {
 
-// Node tiles are TILE_XY x TILE_XY x TILE_Z nodes.  The P2G scatter assigns one
-// 16-lane half-warp to each halo cell column of a tile: TILE_Z + 2 = 16 cells.
-constexpr int TILE_Z = 14;
-constexpr int COL_CELLS = TILE_Z + 2;
+// Node tiles are TILE_XY x TILE_XY x TILE_Z nodes (z fastest inside a tile).
+constexpr int TILE_Z = 16;
 
 // Per-scene data derived on the host from MpmScene.
 struct SceneAux {
@@ -33,8 +31,11 @@ struct Ctx {
     const int* tile_scene;       // scene of each tile
     int* status;                 // device status word (MPM_* bits)
     unsigned long long* fallbacks;  // FP32 Hencky evaluations redone in FP64
-    int* cell_first;             // first sorted slot of an occupied cell (0 if empty)
-    int* cell_last;              // one past its last slot (0 if empty)
+    int* cell_seg;               // dense over padded cells: 1 + segment id of an occupied cell, 0 if empty
+    int* seg_first;              // per segment (occupied cell, sorted order): first sorted slot
+    int* seg_last;               // one past its last slot
+    int* n_seg;                  // number of segments
+    unsigned* blk_count;         // per-block segment counts of the segment scan
     int* tile_flag;              // 1 if the tile receives mass this step
     const void* phi;             // growth field phi_p (growth_mode 1), may be null
     long long n;

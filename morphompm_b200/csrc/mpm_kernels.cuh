@@ -1,26 +1,24 @@
 // Kernels of one MLS-MPM growth step and of its reverse.
 //
 // Forward (python/morphompm/transfer.py:33-79):
-//   bin_kernel       cell key of every particle (stencil base, exact rounding)
-//   radix sort       (sort.cuh) cell-sorted particle order, deterministic
-//   mark_kernel      first/last sorted slot of every occupied cell, tile flags
-//   compact_tiles    active node tiles -> compact grid slots
-//   prepass_kernel   stress and the P2G payload of every particle, sorted order
-//   scatter_kernel   P2G into a node tile, fixed summation order, + grid update
-//   g2p_kernel       gather, advect, F update; clears the cell marks
+//   bin_kernel        cell key of every particle (stencil base, exact rounding)
+//   radix sort        (sort.cuh) cell-sorted particle order, deterministic
+//   seg_* kernels     segment table of the occupied cells + active tile flags
+//   compact_tiles     active node tiles -> compact grid slots
+//   prepass_kernel    stress and the P2G payload of every particle, sorted order
+//   cell_sums_kernel  P2G phase 1: per occupied cell, its 27 stencil sums
+//   node_sums_kernel  P2G phase 2: per node, the sums of its 27 source cells
+//                     in a fixed order, + grid update with boundary conditions
+//   g2p_kernel        gather, advect, F update; clears the cell marks
 // Reverse (python/morphompm/transfer.py:82-158):
 //   bwd_payload_kernel   G2P adjoint payload (nv_b, Cn_b') per particle
-//   scatter_kernel<1>    gv_b scatter + grid adjoint (gmom_b, gm_b)
+//   cell/node_sums<1>    gv_b scatter + grid adjoint (gmom_b, gm_b)
 //   bwd_particle_kernel  P2G adjoint, constitutive VJP, volume path, x_b terms
 //
-// P2G determinism: particles are sorted by cell; a CTA owns one node tile and
-// reads every cell of the tile's 2-cell halo.  A 16-lane half-warp takes one
-// cell column (lane = cell), each lane accumulates its cell's particles in
-// registers, and the column adds its sums into the shared-memory node tile.
-// Columns are processed in 9 colour rounds ((x mod 3, y mod 3) of the column),
-// so within a round no two columns touch the same node, and inside a column the
-// three z-offsets are written in order between __syncwarp()s.  Every node thus
-// sums its contributions in one fixed order and no global atomics are used.
+// P2G determinism: particles are sorted by cell, every occupied cell's sums
+// are formed by one thread in sorted particle order, and every node adds its
+// source cells in the fixed order of the stencil offsets.  No atomics, no
+// shared-memory races: the result does not depend on scheduling.
 #pragma once
 
 #include "mpm_common.cuh"
@@ -155,8 +153,16 @@ __global__ void bin_keys_single(MpmScene sc, long long n, const R* __restrict__ 
 }
 
 // ---------------------------------------------------------------------------
-// cell marks and tile flags
+// segment tables: one segment per occupied cell (a run of equal sorted keys).
+// Three kernels: per-block counts of segment starts (and tile flags), a
+// single-block scan of the counts, and the writes of seg_first / seg_last /
+// cell_seg with each slot's segment id from the scan.  "Outside" keys (stencil
+// entirely off the grid) form no segment.
 // ---------------------------------------------------------------------------
+constexpr int SEG_THREADS = 256;
+constexpr int SEG_ITEMS = 16;
+constexpr int SEG_TILE = SEG_THREADS * SEG_ITEMS;
+
 __device__ __forceinline__ void decode_cell(const MpmScene& sc, long long c, int cell[3]) {
     long long P1 = sc.shape[1] + 2, P2 = sc.shape[2] + 2;
     cell[2] = (int)(c % P2);
@@ -165,38 +171,127 @@ __device__ __forceinline__ void decode_cell(const MpmScene& sc, long long c, int
     cell[0] = (int)(r / P1);
 }
 
-__global__ void __launch_bounds__(256)
-mark_kernel(Ctx ctx, const unsigned* __restrict__ skeys, int flag_tiles) {
-    long long sidx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (sidx >= ctx.n) return;
-    unsigned k = skeys[sidx];
-    bool first = sidx == 0 || skeys[sidx - 1] != k;
-    bool last = sidx == ctx.n - 1 || skeys[sidx + 1] != k;
-    if (!first && !last) return;
-    int s = ctx.scene_of[sidx];
-    const SceneAux& ax = ctx.aux[s];
-    long long c = (long long)k - ax.cell_begin;
-    if (c >= ax.ncells) return;     // outside key
-    if (first) ctx.cell_first[k] = (int)sidx;
-    if (last) ctx.cell_last[k] = (int)(sidx + 1);
-    if (first && flag_tiles) {
-        const MpmScene& sc = ctx.scenes[s];
-        int cell[3];
-        decode_cell(sc, c, cell);
-        int tlo[3], thi[3];
-        const int T[3] = {ctx.tile_xy, ctx.tile_xy, TILE_Z};
+// is slot s the start of an inside segment?
+__device__ __forceinline__ bool seg_start(const Ctx& ctx, const unsigned* __restrict__ skeys, long long s,
+                                          unsigned k) {
+    if (s > 0 && skeys[s - 1] == k) return false;
+    const SceneAux& ax = ctx.aux[ctx.scene_of[s]];
+    return (long long)k - ax.cell_begin < ax.ncells;
+}
+
+__device__ __forceinline__ void flag_tiles(const Ctx& ctx, long long s, unsigned k) {
+    const int sc_i = ctx.scene_of[s];
+    const MpmScene& sc = ctx.scenes[sc_i];
+    const SceneAux& ax = ctx.aux[sc_i];
+    int cell[3];
+    decode_cell(sc, (long long)k - ax.cell_begin, cell);
+    int tlo[3], thi[3];
+    const int T[3] = {ctx.tile_xy, ctx.tile_xy, TILE_Z};
 #pragma unroll
-        for (int d = 0; d < 3; ++d) {
-            int b = cell[d] - 2;
-            int lo = b < 0 ? 0 : b;
-            int hi = b + 2 > sc.shape[d] - 1 ? sc.shape[d] - 1 : b + 2;
-            tlo[d] = lo / T[d];
-            thi[d] = hi / T[d];
+    for (int d = 0; d < 3; ++d) {
+        int b = cell[d] - 2;
+        int lo = b < 0 ? 0 : b;
+        int hi = b + 2 > sc.shape[d] - 1 ? sc.shape[d] - 1 : b + 2;
+        tlo[d] = lo / T[d];
+        thi[d] = hi / T[d];
+    }
+    for (int a = tlo[0]; a <= thi[0]; ++a)
+        for (int b = tlo[1]; b <= thi[1]; ++b)
+            for (int e = tlo[2]; e <= thi[2]; ++e)
+                ctx.tile_flag[ax.tile_begin + ((long long)a * ax.ntile[1] + b) * ax.ntile[2] + e] = 1;
+}
+
+__global__ void __launch_bounds__(SEG_THREADS)
+seg_count_kernel(Ctx ctx, const unsigned* __restrict__ skeys, int flag) {
+    __shared__ unsigned red[SEG_THREADS];
+    const long long base = (long long)blockIdx.x * SEG_TILE + (long long)threadIdx.x * SEG_ITEMS;
+    unsigned cnt = 0;
+#pragma unroll 4
+    for (int i = 0; i < SEG_ITEMS; ++i) {
+        long long s = base + i;
+        if (s >= ctx.n) break;
+        unsigned k = skeys[s];
+        if (seg_start(ctx, skeys, s, k)) {
+            ++cnt;
+            if (flag) flag_tiles(ctx, s, k);
         }
-        for (int a = tlo[0]; a <= thi[0]; ++a)
-            for (int b = tlo[1]; b <= thi[1]; ++b)
-                for (int e = tlo[2]; e <= thi[2]; ++e)
-                    ctx.tile_flag[ax.tile_begin + ((long long)a * ax.ntile[1] + b) * ax.ntile[2] + e] = 1;
+    }
+    red[threadIdx.x] = cnt;
+    __syncthreads();
+    for (int w = SEG_THREADS / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) ctx.blk_count[blockIdx.x] = red[0];
+}
+
+// exclusive scan of the block counts in place; total -> *n_seg (single block)
+__global__ void __launch_bounds__(1024)
+seg_scan_kernel(Ctx ctx, int nblk) {
+    __shared__ unsigned sh[1024];
+    __shared__ unsigned carry;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    for (int b0 = 0; b0 < nblk; b0 += 1024) {
+        int b = b0 + threadIdx.x;
+        unsigned v = b < nblk ? ctx.blk_count[b] : 0u;
+        sh[threadIdx.x] = v;
+        __syncthreads();
+        for (int o = 1; o < 1024; o <<= 1) {
+            unsigned t = threadIdx.x >= (unsigned)o ? sh[threadIdx.x - o] : 0u;
+            __syncthreads();
+            sh[threadIdx.x] += t;
+            __syncthreads();
+        }
+        unsigned c = carry;
+        if (b < nblk) ctx.blk_count[b] = c + sh[threadIdx.x] - v;
+        __syncthreads();
+        if (threadIdx.x == 1023) carry = c + sh[1023];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *ctx.n_seg = (int)carry;
+}
+
+__global__ void __launch_bounds__(SEG_THREADS)
+seg_write_kernel(Ctx ctx, const unsigned* __restrict__ skeys) {
+    __shared__ unsigned sh[SEG_THREADS];
+    const long long base = (long long)blockIdx.x * SEG_TILE + (long long)threadIdx.x * SEG_ITEMS;
+    unsigned cnt = 0;
+    unsigned flags = 0;
+#pragma unroll
+    for (int i = 0; i < SEG_ITEMS; ++i) {
+        long long s = base + i;
+        if (s < ctx.n && seg_start(ctx, skeys, s, skeys[s])) {
+            ++cnt;
+            flags |= 1u << i;
+        }
+    }
+    sh[threadIdx.x] = cnt;
+    __syncthreads();
+    for (int o = 1; o < SEG_THREADS; o <<= 1) {
+        unsigned t = threadIdx.x >= (unsigned)o ? sh[threadIdx.x - o] : 0u;
+        __syncthreads();
+        sh[threadIdx.x] += t;
+        __syncthreads();
+    }
+    // segments started before this thread's first slot
+    unsigned run = ctx.blk_count[blockIdx.x] + sh[threadIdx.x] - cnt;
+#pragma unroll 4
+    for (int i = 0; i < SEG_ITEMS; ++i) {
+        long long s = base + i;
+        if (s >= ctx.n) break;
+        unsigned k = skeys[s];
+        if (flags & (1u << i)) {
+            ctx.seg_first[run] = (int)s;
+            ctx.cell_seg[k] = (int)run + 1;
+            ++run;
+        }
+        bool last = s == ctx.n - 1 || skeys[s + 1] != k;
+        if (last && run > 0) {
+            // the slot belongs to segment run-1 only if its key is inside
+            const SceneAux& ax = ctx.aux[ctx.scene_of[s]];
+            if ((long long)k - ax.cell_begin < ax.ncells) ctx.seg_last[run - 1] = (int)(s + 1);
+        }
     }
 }
 
@@ -240,26 +335,119 @@ prepass_kernel(Ctx ctx, MpmParticles P, const unsigned* __restrict__ perm, R* __
 }
 
 // ---------------------------------------------------------------------------
-// P2G scatter into one node tile per CTA iteration (see file header).
-// MODE 0: channels (m, mom[3]); epilogue = grid update -> (m, v[3]).
-// MODE 1: channels (gv_b[3]);  epilogue = grid adjoint -> (gm_b, gmom_b[3]).
-// OXB: stencil x-offsets accumulated per pass over a cell's particles.
+// P2G, phase 1: per-cell sums.  One thread per segment (occupied cell) adds
+// its particles' contributions to the 27 stencil nodes, in sorted order, in
+// registers, and stores them as sums[o][segment] (o = 9 ox + 3 oy + oz).
+// MODE 0: channels (m, mom[3]);  MODE 1: channels (gv_b[3], unused).
+// OXB: stencil x-offsets accumulated per pass over the cell's particles.
 // ---------------------------------------------------------------------------
-template <typename R, int T, int MODE, int OXB>
+template <typename R>
+__device__ __forceinline__ void store_sum(R* __restrict__ S, long long idx, const R v[4]) {
+    if constexpr (sizeof(R) == 4) {
+        reinterpret_cast<float4*>(S)[idx] = make_float4(v[0], v[1], v[2], v[3]);
+    } else {
+        double2* p = reinterpret_cast<double2*>(S) + 2 * idx;
+        p[0] = make_double2(v[0], v[1]);
+        p[1] = make_double2(v[2], v[3]);
+    }
+}
+
+template <typename R, int MODE, int OXB>
+__global__ void __launch_bounds__(128)
+cell_sums_kernel(Ctx ctx, const R* __restrict__ payload, R* __restrict__ S, long long cap) {
+    const int nseg = *ctx.n_seg;
+    for (int id = blockIdx.x * blockDim.x + threadIdx.x; id < nseg; id += gridDim.x * blockDim.x) {
+        const int first = ctx.seg_first[id], last = ctx.seg_last[id];
+#pragma unroll 1
+        for (int ox0 = 0; ox0 < 3; ox0 += OXB) {
+            R acc[OXB][3][3][4];
+#pragma unroll
+            for (int a = 0; a < OXB; ++a)
+#pragma unroll
+                for (int b = 0; b < 3; ++b)
+#pragma unroll
+                    for (int c = 0; c < 3; ++c)
+#pragma unroll
+                        for (int h = 0; h < 4; ++h) acc[a][b][c][h] = R(0);
+            for (int q = first; q < last; ++q) {
+                R r[PAYLOAD];
+                load_record(payload, q, r);
+                R w[3][3];
+                bspline(r, w);
+                R dz[3] = {R(0) - r[2], R(1) - r[2], R(2) - r[2]};
+                R dy[3] = {R(0) - r[1], R(1) - r[1], R(2) - r[1]};
+#pragma unroll
+                for (int a = 0; a < OXB; ++a) {
+                    const int ox = ox0 + a;
+                    const R dpx = R(ox) - r[0];
+                    R wx;
+                    if constexpr (OXB == 3) wx = w[a][0];
+                    else wx = ox == 0 ? w[0][0] : (ox == 1 ? w[1][0] : w[2][0]);
+                    // a + B dp with dp = (dpx, dy, dz), x part hoisted
+                    const R ax0 = r[4] + r[7] * dpx, ax1 = r[5] + r[10] * dpx, ax2 = r[6] + r[13] * dpx;
+#pragma unroll
+                    for (int oy = 0; oy < 3; ++oy) {
+                        const R wxy = wx * w[oy][1];
+                        const R ay0 = ax0 + r[8] * dy[oy], ay1 = ax1 + r[11] * dy[oy], ay2 = ax2 + r[14] * dy[oy];
+#pragma unroll
+                        for (int oz = 0; oz < 3; ++oz) {
+                            const R wt = wxy * w[oz][2];
+                            const R q0 = ay0 + r[9] * dz[oz];
+                            const R q1 = ay1 + r[12] * dz[oz];
+                            const R q2 = ay2 + r[15] * dz[oz];
+                            if constexpr (MODE == 0) {
+                                acc[a][oy][oz][0] += wt * r[3];
+                                acc[a][oy][oz][1] += wt * q0;
+                                acc[a][oy][oz][2] += wt * q1;
+                                acc[a][oy][oz][3] += wt * q2;
+                            } else {
+                                acc[a][oy][oz][0] += wt * q0;
+                                acc[a][oy][oz][1] += wt * q1;
+                                acc[a][oy][oz][2] += wt * q2;
+                            }
+                        }
+                    }
+                }
+            }
+#pragma unroll
+            for (int a = 0; a < OXB; ++a)
+#pragma unroll
+                for (int oy = 0; oy < 3; ++oy)
+#pragma unroll
+                    for (int oz = 0; oz < 3; ++oz) {
+                        const int o = 9 * (ox0 + a) + 3 * oy + oz;
+                        store_sum(S, (long long)o * cap + id, acc[a][oy][oz]);
+                    }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// P2G, phase 2: node gather + grid update.  One CTA per active node tile
+// (persistent over the active list); every node adds the sums of its 27
+// source cells in the fixed order o = 0..26, then
+// MODE 0: grid update -> (m, v[3]) with v = s mom/m + s dt g on free nodes;
+// MODE 1: grid adjoint -> (gm_b, gmom_b[3]) from gv_b and the forward record.
+// ---------------------------------------------------------------------------
+template <typename R>
+__device__ __forceinline__ void load_sum(const R* __restrict__ S, long long idx, R o[4]) {
+    if constexpr (sizeof(R) == 4) {
+        float4 v = __ldg(reinterpret_cast<const float4*>(S) + idx);
+        o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = v.w;
+    } else {
+        const double2* p = reinterpret_cast<const double2*>(S) + 2 * idx;
+        double2 a = __ldg(p), b = __ldg(p + 1);
+        o[0] = a.x; o[1] = a.y; o[2] = b.x; o[3] = b.y;
+    }
+}
+
+template <typename R, int T, int MODE>
 __global__ void __launch_bounds__(256)
-scatter_kernel(Ctx ctx, const R* __restrict__ payload, const int* __restrict__ active,
-               const int* __restrict__ n_active, R* __restrict__ grid_out, const R* __restrict__ grid_fwd,
-               int advect) {
+node_sums_kernel(Ctx ctx, const R* __restrict__ S, long long cap, const int* __restrict__ active,
+                 const int* __restrict__ n_active, R* __restrict__ grid_out, const R* __restrict__ grid_fwd,
+                 int advect) {
     constexpr int TN = T * T * TILE_Z;
-    constexpr int NCH = MODE == 0 ? 4 : 3;
-    constexpr int HALO = T + 2;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    R* acc_s = reinterpret_cast<R*>(smem_raw);   // [NCH][TN]
-
-    const int grp = threadIdx.x >> 4;   // 16 column groups
-    const int l = threadIdx.x & 15;     // cell within the column
     const int nact = *n_active;
-
     for (int it = blockIdx.x; it < nact; it += gridDim.x) {
         const int tile = active[it];
         const int s = ctx.tile_scene[tile];
@@ -270,100 +458,7 @@ scatter_kernel(Ctx ctx, const R* __restrict__ payload, const int* __restrict__ a
         const int ty = (int)((lt / ax.ntile[2]) % ax.ntile[1]);
         const int tx = (int)(lt / ((long long)ax.ntile[2] * ax.ntile[1]));
         const int L0 = tx * T, L1 = ty * T, L2 = tz * TILE_Z;
-        const int P0 = sc.shape[0] + 2, P1 = sc.shape[1] + 2, P2 = sc.shape[2] + 2;
-
-        for (int i = threadIdx.x; i < NCH * TN; i += blockDim.x) acc_s[i] = R(0);
-        __syncthreads();
-
-        for (int color = 0; color < 9; ++color) {
-            const int ca = color / 3, cb = color % 3;
-            const int ncy = (HALO - cb + 2) / 3;
-            const int ncol = ((HALO - ca + 2) / 3) * ncy;
-            for (int c0 = 0; c0 < ncol; c0 += 16) {
-                const int col = c0 + grp;
-                int first = 0, last = 0, hx = 0, hy = 0;
-                if (col < ncol) {
-                    hx = ca + 3 * (col / ncy);
-                    hy = cb + 3 * (col % ncy);
-                    const int cx = L0 + hx, cy = L1 + hy, cz = L2 + l;
-                    if (cx < P0 && cy < P1 && cz < P2) {
-                        long long key = ax.cell_begin + ((long long)cx * P1 + cy) * P2 + cz;
-                        first = ctx.cell_first[key];
-                        last = ctx.cell_last[key];
-                    }
-                }
-#pragma unroll 1
-                for (int ox0 = 0; ox0 < 3; ox0 += OXB) {
-                    R acc[OXB][3][3][NCH];
-#pragma unroll
-                    for (int a = 0; a < OXB; ++a)
-#pragma unroll
-                        for (int b = 0; b < 3; ++b)
-#pragma unroll
-                            for (int c = 0; c < 3; ++c)
-#pragma unroll
-                                for (int h = 0; h < NCH; ++h) acc[a][b][c][h] = R(0);
-                    for (int q = first; q < last; ++q) {
-                        R r[PAYLOAD];
-                        load_record(payload, q, r);
-                        R w[3][3];
-                        bspline(r, w);
-#pragma unroll
-                        for (int a = 0; a < OXB; ++a) {
-                            const int ox = ox0 + a;
-                            const R dpx = R(ox) - r[0];
-                            const R wx = w[ox][0];
-#pragma unroll
-                            for (int oy = 0; oy < 3; ++oy) {
-                                const R dpy = R(oy) - r[1];
-                                const R wxy = wx * w[oy][1];
-#pragma unroll
-                                for (int oz = 0; oz < 3; ++oz) {
-                                    const R dpz = R(oz) - r[2];
-                                    const R wt = wxy * w[oz][2];
-                                    R q0 = r[4] + r[7] * dpx + r[8] * dpy + r[9] * dpz;
-                                    R q1 = r[5] + r[10] * dpx + r[11] * dpy + r[12] * dpz;
-                                    R q2 = r[6] + r[13] * dpx + r[14] * dpy + r[15] * dpz;
-                                    if constexpr (MODE == 0) {
-                                        acc[a][oy][oz][0] += wt * r[3];
-                                        acc[a][oy][oz][1] += wt * q0;
-                                        acc[a][oy][oz][2] += wt * q1;
-                                        acc[a][oy][oz][3] += wt * q2;
-                                    } else {
-                                        acc[a][oy][oz][0] += wt * q0;
-                                        acc[a][oy][oz][1] += wt * q1;
-                                        acc[a][oy][oz][2] += wt * q2;
-                                    }
-                                }
-                            }
-                        }
-                    }
-                    const bool has = last > first;
-#pragma unroll
-                    for (int a = 0; a < OXB; ++a) {
-                        const int nx = hx - 2 + ox0 + a;
-#pragma unroll
-                        for (int oz = 0; oz < 3; ++oz) {
-                            __syncwarp();
-                            const int nz = l - 2 + oz;
-#pragma unroll
-                            for (int oy = 0; oy < 3; ++oy) {
-                                const int ny = hy - 2 + oy;
-                                if (has && nx >= 0 && nx < T && ny >= 0 && ny < T && nz >= 0 && nz < TILE_Z) {
-                                    const int node = (nx * T + ny) * TILE_Z + nz;
-#pragma unroll
-                                    for (int h = 0; h < NCH; ++h) acc_s[h * TN + node] += acc[a][oy][oz][h];
-                                }
-                            }
-                        }
-                        __syncwarp();
-                    }
-                }
-            }
-            __syncthreads();
-        }
-
-        // epilogue: node tile -> compact grid records
+        const long long P1 = sc.shape[1] + 2, P2 = sc.shape[2] + 2;
         const R s_damp = (R)(1.0 - sc.damping);
         const R dt = (R)sc.dt;
         const R eps = (R)sc.mass_eps;
@@ -372,70 +467,104 @@ scatter_kernel(Ctx ctx, const R* __restrict__ payload, const int* __restrict__ a
             const int nz = node % TILE_Z, ny = (node / TILE_Z) % T, nx = node / (TILE_Z * T);
             const int i = L0 + nx, j = L1 + ny, k = L2 + nz;
             if (i >= sc.shape[0] || j >= sc.shape[1] || k >= sc.shape[2]) continue;
+            R acc[4] = {R(0), R(0), R(0), R(0)};
+            // source cell of offset o is padded cell (i,j,k) + 2 - o
+            const long long cbase = ax.cell_begin + ((long long)(i + 2) * P1 + (j + 2)) * P2 + (k + 2);
+#pragma unroll
+            for (int ox = 0; ox < 3; ++ox)
+#pragma unroll
+                for (int oy = 0; oy < 3; ++oy)
+#pragma unroll
+                    for (int oz = 0; oz < 3; ++oz) {
+                        const int id1 = ctx.cell_seg[cbase - ((long long)ox * P1 + oy) * P2 - oz];
+                        if (id1) {
+                            R v[4];
+                            load_sum(S, (long long)(9 * ox + 3 * oy + oz) * cap + (id1 - 1), v);
+                            acc[0] += v[0]; acc[1] += v[1]; acc[2] += v[2]; acc[3] += v[3];
+                        }
+                    }
             const long long gidx = (long long)it * TN + node;
-            R rec[4];
+            R rec[4] = {R(0), R(0), R(0), R(0)};
             if constexpr (MODE == 0) {
-                const R m = acc_s[node];
-                rec[0] = m; rec[1] = R(0); rec[2] = R(0); rec[3] = R(0);
+                const R m = acc[0];
+                rec[0] = m;
                 if (m > eps && node_free(sc, i, j, k)) {
-                    rec[1] = (s_damp * acc_s[TN + node]) / m + s_damp * dt * g0;
-                    rec[2] = (s_damp * acc_s[2 * TN + node]) / m + s_damp * dt * g1;
-                    rec[3] = (s_damp * acc_s[3 * TN + node]) / m + s_damp * dt * g2;
+                    rec[1] = (s_damp * acc[1]) / m + s_damp * dt * g0;
+                    rec[2] = (s_damp * acc[2]) / m + s_damp * dt * g1;
+                    rec[3] = (s_damp * acc[3]) / m + s_damp * dt * g2;
                 }
             } else {
                 R f[4];
                 load_node(grid_fwd, gidx, f);
-                rec[0] = R(0); rec[1] = R(0); rec[2] = R(0); rec[3] = R(0);
                 const R m = f[0];
                 if (m > eps && node_free(sc, i, j, k)) {
-                    const R b0 = acc_s[node], b1 = acc_s[TN + node], b2 = acc_s[2 * TN + node];
-                    rec[1] = (s_damp * b0) / m;
-                    rec[2] = (s_damp * b1) / m;
-                    rec[3] = (s_damp * b2) / m;
+                    rec[1] = (s_damp * acc[0]) / m;
+                    rec[2] = (s_damp * acc[1]) / m;
+                    rec[3] = (s_damp * acc[2]) / m;
                     if (advect) {
                         const R sd = s_damp * dt;
-                        rec[0] = -(b0 * (f[1] - sd * g0) + b1 * (f[2] - sd * g1) + b2 * (f[3] - sd * g2)) / m;
+                        rec[0] = -(acc[0] * (f[1] - sd * g0) + acc[1] * (f[2] - sd * g1) + acc[2] * (f[3] - sd * g2)) / m;
                     }
                 }
             }
             store_node(grid_out, gidx, rec);
         }
-        __syncthreads();
     }
 }
 
 // ---------------------------------------------------------------------------
-// stencil addressing into the compact per-tile grid
+// stencil addressing into the compact per-tile grid.  A particle's 3x3x3
+// stencil spans at most 2 tiles per axis; the (up to 8) tile slots are looked
+// up once, then every node record index is slot*TN + local.
 // ---------------------------------------------------------------------------
 template <int T>
 struct Stencil {
-    int node[3][3];     // node index per axis and offset (-1 if out of range)
-    int tl[3][3];       // tile coordinate
-    int lc[3][3];       // coordinate inside the tile
-    __device__ __forceinline__ void init(const MpmScene& sc, const int base[3]) {
+    int lc[3][3];       // coordinate inside the tile, per axis and offset
+    int sel[3][3];      // 0: first tile of the axis, 1: second, -1: node off the grid
+    long long s000, s001, s010, s011, s100, s101, s110, s111;   // tile slots (-1 missing)
+    __device__ __forceinline__ void init(const Ctx& ctx, const MpmScene& sc, const SceneAux& ax,
+                                         const int* __restrict__ tile_slot, const int base[3]) {
         const int TT[3] = {T, T, TILE_Z};
+        int t0[3], t1[3];
 #pragma unroll
-        for (int d = 0; d < 3; ++d)
+        for (int d = 0; d < 3; ++d) {
+            int lo = base[d] < 0 ? 0 : base[d];
+            t0[d] = lo / TT[d];
+            t1[d] = t0[d];
 #pragma unroll
             for (int o = 0; o < 3; ++o) {
                 int n = base[d] + o;
                 bool ok = n >= 0 && n < sc.shape[d];
-                node[d][o] = ok ? n : -1;
-                int t = ok ? n / TT[d] : 0;
-                tl[d][o] = t;
+                int t = ok ? n / TT[d] : t0[d];
+                if (ok && t != t0[d]) t1[d] = t;
+                sel[d][o] = ok ? (t == t0[d] ? 0 : 1) : -1;
                 lc[d][o] = ok ? n - t * TT[d] : 0;
             }
+        }
+        auto look = [&](int a, int b, int c) -> long long {
+            int tx = a ? t1[0] : t0[0], ty = b ? t1[1] : t0[1], tz = c ? t1[2] : t0[2];
+            bool need = (a == 0 || t1[0] != t0[0]) && (b == 0 || t1[1] != t0[1]) && (c == 0 || t1[2] != t0[2]);
+            if (!need || tx >= ax.ntile[0] || ty >= ax.ntile[1] || tz >= ax.ntile[2]) return -1;
+            return tile_slot[ax.tile_begin + ((long long)tx * ax.ntile[1] + ty) * ax.ntile[2] + tz];
+        };
+        s000 = look(0, 0, 0); s001 = look(0, 0, 1); s010 = look(0, 1, 0); s011 = look(0, 1, 1);
+        s100 = look(1, 0, 0); s101 = look(1, 0, 1); s110 = look(1, 1, 0); s111 = look(1, 1, 1);
     }
     // compact record index or -1
-    __device__ __forceinline__ long long rec(const Ctx& ctx, const SceneAux& ax, const int* __restrict__ tile_slot,
-                                             int a, int b, int c) const {
-        if (node[0][a] < 0 || node[1][b] < 0 || node[2][c] < 0) return -1;
-        long long tile = ax.tile_begin + ((long long)tl[0][a] * ax.ntile[1] + tl[1][b]) * ax.ntile[2] + tl[2][c];
-        int slot = tile_slot[tile];
-        if (slot < 0) return -1;
-        return (long long)slot * (T * T * TILE_Z) + (lc[0][a] * T + lc[1][b]) * TILE_Z + lc[2][c];
+    __device__ __forceinline__ long long rec(int a, int b, int c) const {
+        const int x = sel[0][a], y = sel[1][b], z = sel[2][c];
+        if (x < 0 || y < 0 || z < 0) return -1;
+        long long sl = x ? (y ? (z ? s111 : s110) : (z ? s101 : s100)) : (y ? (z ? s011 : s010) : (z ? s001 : s000));
+        if (sl < 0) return -1;
+        return sl * (T * T * TILE_Z) + (lc[0][a] * T + lc[1][b]) * TILE_Z + lc[2][c];
     }
 };
+
+__device__ __forceinline__ void unmark_cell(const Ctx& ctx, const SceneAux& ax, const unsigned* __restrict__ skeys,
+                                            long long sidx) {
+    unsigned k = skeys[sidx];
+    if ((sidx == 0 || skeys[sidx - 1] != k) && (long long)k - ax.cell_begin < ax.ncells) ctx.cell_seg[k] = 0;
+}
 
 // ---------------------------------------------------------------------------
 // G2P + advection + F update (transfer.py:61-79); writes the output state in
@@ -452,16 +581,15 @@ g2p_kernel(Ctx ctx, Tape<R> tp, MpmParticles in, MpmParticles out, int advect) {
     const SceneAux& ax = ctx.aux[s];
     const R dx = (R)sc.dx, dt = (R)sc.dt, inv_dx = (R)(1.0 / sc.dx);
     const R k4 = R(4) * inv_dx * inv_dx;
-    R x[3], F[9];
+    R x[3];
     ld3<R>(in.x, p, in.sp3, in.sc3, x);
-    ld9<R>(in.F, p, in.sp9, in.sc9, F);
     int base[3];
     R fx[3];
     bin_particle(x, inv_dx, sc.shape, base, fx);
     R w[3][3];
     bspline(fx, w);
     Stencil<T> st;
-    st.init(sc, base);
+    st.init(ctx, sc, ax, tp.tile_slot, base);
     R nv[3] = {0, 0, 0}, nC[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
 #pragma unroll
     for (int a = 0; a < 3; ++a)
@@ -469,7 +597,7 @@ g2p_kernel(Ctx ctx, Tape<R> tp, MpmParticles in, MpmParticles out, int advect) {
         for (int b = 0; b < 3; ++b)
 #pragma unroll
             for (int c = 0; c < 3; ++c) {
-                long long r = st.rec(ctx, ax, tp.tile_slot, a, b, c);
+                long long r = st.rec(a, b, c);
                 if (r < 0) continue;
                 R g[4];
                 load_node(tp.grid, r, g);
@@ -483,6 +611,8 @@ g2p_kernel(Ctx ctx, Tape<R> tp, MpmParticles in, MpmParticles out, int advect) {
                     for (int j = 0; j < 3; ++j) nC[3 * i + j] += kw * (g[1 + i] * dp[j]);
                 }
             }
+    R F[9];
+    ld9<R>(in.F, p, in.sp9, in.sc9, F);
     R xn[3];
 #pragma unroll
     for (int i = 0; i < 3; ++i) xn[i] = advect ? x[i] + dt * nv[i] : x[i];
@@ -501,14 +631,7 @@ g2p_kernel(Ctx ctx, Tape<R> tp, MpmParticles in, MpmParticles out, int advect) {
     }
     if (!finite9(Fn) || !(xn[0] * R(0) == R(0) && xn[1] * R(0) == R(0) && xn[2] * R(0) == R(0)))
         raise_status(ctx.status, MPM_ERR_NONFINITE);
-    // clear this step's cell marks
-    unsigned k = tp.skeys[sidx];
-    if (sidx == 0 || tp.skeys[sidx - 1] != k) {
-        if ((long long)k - ax.cell_begin < ax.ncells) {
-            ctx.cell_first[k] = 0;
-            ctx.cell_last[k] = 0;
-        }
-    }
+    unmark_cell(ctx, ax, tp.skeys, sidx);
 }
 
 // ---------------------------------------------------------------------------
@@ -548,7 +671,11 @@ bwd_payload_kernel(Ctx ctx, const unsigned* __restrict__ perm, MpmParticles in, 
 }
 
 // ---------------------------------------------------------------------------
-// reverse: per-particle cotangents (transfer.py:99-119 x_b terms, 129-156)
+// reverse: per-particle cotangents (transfer.py:99-119 x_b terms, 129-156).
+// The x_b terms of the reference are regrouped per node as
+//   x_b += [nv_b.gv + pm mb.v + pm gm_b + (M1 gv + M2 mb).dp] dW
+// with M1 = k4 Cn_b'^T, M2 = pm C^T + dt sk^T, and the weight-only terms are
+// summed once per particle: x_b -= M1 sum(w gv) + M2 sum(w mb).
 // ---------------------------------------------------------------------------
 template <typename R, int T>
 __global__ void __launch_bounds__(256)
@@ -565,105 +692,109 @@ bwd_particle_kernel(Ctx ctx, Tape<R> tp, const R* __restrict__ gridb, MpmParticl
     const R dx = (R)sc.dx, dt = (R)sc.dt, inv_dx = (R)(1.0 / sc.dx);
     const R k4 = R(4) * inv_dx * inv_dx;
     const R pm = (R)sc.pmass;
-    R x[3], v[3], C[9], F[9], Fg[9], Cn[9];
+    R x[3], C[9], F[9], Fg[9];
     R gphi;
     ld3<R>(in.x, p, in.sp3, in.sc3, x);
-    ld3<R>(in.v, p, in.sp3, in.sc3, v);
     ld9<R>(in.C, p, in.sp9, in.sc9, C);
     ld9<R>(in.F, p, in.sp9, in.sc9, F);
     load_Fg<R>(ctx, sc, in, p, t, Fg, &gphi);
-    ld9<R>(outC, p, in.sp9, in.sc9, Cn);
-    R xnb[3], vnb[3], Cnb_in[9], Fnb[9];
-    ld3<R>(ob.x, p, ob.sp3, ob.sc3, xnb);
-    ld3<R>(ob.v, p, ob.sp3, ob.sc3, vnb);
-    ld9<R>(ob.C, p, ob.sp9, ob.sc9, Cnb_in);
-    ld9<R>(ob.F, p, ob.sp9, ob.sc9, Fnb);
 
+    R tau[9];
+    bool fb = model_stress(M, ctx.gap_thresh, F, Fg, C, tau);
+    const R c = -k4 * (R)sc.vol0 * det3(Fg);
+
+    // per-particle matrices of the regrouped x_b terms
+    R M1[9], M2[9], nvb[3], pv[3];
+    {
+        R xnb[3], vnb[3], Cnb[9], Fnb[9], v[3];
+        ld3<R>(ob.x, p, ob.sp3, ob.sc3, xnb);
+        ld3<R>(ob.v, p, ob.sp3, ob.sc3, vnb);
+        ld9<R>(ob.C, p, ob.sp9, ob.sc9, Cnb);
+        ld9<R>(ob.F, p, ob.sp9, ob.sc9, Fnb);
+        ld3<R>(in.v, p, in.sp3, in.sc3, v);
+        R FbFt[9];
+        mmT(Fnb, F, FbFt);
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            nvb[i] = advect ? vnb[i] + dt * xnb[i] : vnb[i];
+            pv[i] = pm * v[i];
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+                M1[3 * i + j] = k4 * (Cnb[3 * j + i] + dt * FbFt[3 * j + i]);       // k4 Cn_b'^T
+                M2[3 * i + j] = pm * C[3 * j + i] + dt * (c * tau[3 * j + i]);       // pm C^T + dt sk^T
+            }
+        }
+    }
     int base[3];
     R fx[3];
     bin_particle(x, inv_dx, sc.shape, base, fx);
     R w[3][3], dw[3][3];
     bspline(fx, w);
     bspline_grad(fx, dw);
+    Stencil<T> st;
+    st.init(ctx, sc, ax, tp.tile_slot, base);
 
-    R tau[9];
-    bool fb = model_stress(M, ctx.gap_thresh, F, Fg, C, tau);
-    R c = -k4 * (R)sc.vol0 * det3(Fg);
-    R sk[9];
+    R xb[3] = {0, 0, 0}, wgv[3] = {0, 0, 0}, wmb[3] = {0, 0, 0}, Sb[9];
 #pragma unroll
-    for (int i = 0; i < 9; ++i) sk[i] = c * tau[i];
-
-    R nvb[3], Cnb[9], Fb[9], xb[3], vb[3] = {0, 0, 0}, Sb[9];
+    for (int i = 0; i < 9; ++i) Sb[i] = R(0);
 #pragma unroll
-    for (int i = 0; i < 3; ++i) {
-        nvb[i] = advect ? vnb[i] + dt * xnb[i] : vnb[i];
-        xb[i] = advect ? xnb[i] : R(0);
-    }
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int b = 0; b < 3; ++b)
+#pragma unroll
+            for (int cc = 0; cc < 3; ++cc) {
+                long long r = st.rec(a, b, cc);
+                if (r < 0) continue;
+                R gf[4], gb[4];
+                load_node(tp.grid, r, gf);
+                load_node(gridb, r, gb);
+                const R wa = a == 0 ? w[0][0] : (a == 1 ? w[1][0] : w[2][0]);
+                const R da = a == 0 ? dw[0][0] : (a == 1 ? dw[1][0] : dw[2][0]);
+                const R wt = wa * w[b][1] * w[cc][2];
+                const R dp[3] = {(R(a) - fx[0]) * dx, (R(b) - fx[1]) * dx, (R(cc) - fx[2]) * dx};
+                const R* gv = gf + 1;
+                const R* mb = gb + 1;
+#pragma unroll
+                for (int i = 0; i < 3; ++i) {
+                    wgv[i] += wt * gv[i];
+                    wmb[i] += wt * mb[i];
+#pragma unroll
+                    for (int j = 0; j < 3; ++j) Sb[3 * i + j] += wt * (mb[i] * dp[j]);
+                }
+                if (advect) {
+                    R beta[3];
+#pragma unroll
+                    for (int i = 0; i < 3; ++i)
+                        beta[i] = M1[3 * i] * gv[0] + M1[3 * i + 1] * gv[1] + M1[3 * i + 2] * gv[2]
+                                + M2[3 * i] * mb[0] + M2[3 * i + 1] * mb[1] + M2[3 * i + 2] * mb[2];
+                    const R sfac = nvb[0] * gv[0] + nvb[1] * gv[1] + nvb[2] * gv[2]
+                                 + mb[0] * pv[0] + mb[1] * pv[1] + mb[2] * pv[2] + gb[0] * pm
+                                 + beta[0] * dp[0] + beta[1] * dp[1] + beta[2] * dp[2];
+                    xb[0] += sfac * (da * w[b][1] * w[cc][2] * inv_dx);
+                    xb[1] += sfac * (wa * dw[b][1] * w[cc][2] * inv_dx);
+                    xb[2] += sfac * (wa * w[b][1] * dw[cc][2] * inv_dx);
+                }
+            }
+    R Fb[9], vb[3], Cb[9], skb[9], taub[9];
     {
-        R FbFt[9];
-        mmT(Fnb, F, FbFt);
-#pragma unroll
-        for (int i = 0; i < 9; ++i) Cnb[i] = Cnb_in[i] + dt * FbFt[i];
+        R Cn[9], Fnb[9];
+        ld9<R>(outC, p, in.sp9, in.sc9, Cn);
+        ld9<R>(ob.F, p, ob.sp9, ob.sc9, Fnb);
         R A[9];
 #pragma unroll
         for (int i = 0; i < 9; ++i) A[i] = ((i % 4 == 0) ? R(1) : R(0)) + dt * Cn[i];
         mTm(A, Fnb, Fb);   // (I + dt Cn)^T Fn_b
     }
+    if (advect) {
+        R xnb[3];
+        ld3<R>(ob.x, p, ob.sp3, ob.sc3, xnb);
 #pragma unroll
-    for (int i = 0; i < 9; ++i) Sb[i] = R(0);
-
-    Stencil<T> st;
-    st.init(sc, base);
-#pragma unroll 1
-    for (int a = 0; a < 3; ++a)
-#pragma unroll 1
-        for (int b = 0; b < 3; ++b)
+        for (int i = 0; i < 3; ++i)
+            xb[i] += xnb[i] - (M1[3 * i] * wgv[0] + M1[3 * i + 1] * wgv[1] + M1[3 * i + 2] * wgv[2])
+                   - (M2[3 * i] * wmb[0] + M2[3 * i + 1] * wmb[1] + M2[3 * i + 2] * wmb[2]);
+    }
 #pragma unroll
-            for (int cc = 0; cc < 3; ++cc) {
-                long long r = st.rec(ctx, ax, tp.tile_slot, a, b, cc);
-                if (r < 0) continue;
-                R gf[4], gb[4];
-                load_node(tp.grid, r, gf);
-                load_node(gridb, r, gb);
-                const R wt = w[a][0] * w[b][1] * w[cc][2];
-                const R dp[3] = {(R(a) - fx[0]) * dx, (R(b) - fx[1]) * dx, (R(cc) - fx[2]) * dx};
-                const R* gv = gf + 1;
-                const R* mb = gb + 1;
-                if (advect) {
-                    const R dW[3] = {dw[a][0] * w[b][1] * w[cc][2] * inv_dx, w[a][0] * dw[b][1] * w[cc][2] * inv_dx,
-                                     w[a][0] * w[b][1] * dw[cc][2] * inv_dx};
-                    // G2P adjoint through the weights and dpos
-                    R t1 = nvb[0] * gv[0] + nvb[1] * gv[1] + nvb[2] * gv[2];
-                    R Cd[3];
-#pragma unroll
-                    for (int i = 0; i < 3; ++i) Cd[i] = Cnb[3 * i] * dp[0] + Cnb[3 * i + 1] * dp[1] + Cnb[3 * i + 2] * dp[2];
-                    R t2 = k4 * (gv[0] * Cd[0] + gv[1] * Cd[1] + gv[2] * Cd[2]);
-                    const R kw = k4 * wt;
-#pragma unroll
-                    for (int i = 0; i < 3; ++i)
-                        xb[i] += (t1 + t2) * dW[i] - kw * (Cnb[i] * gv[0] + Cnb[3 + i] * gv[1] + Cnb[6 + i] * gv[2]);
-                    // P2G adjoint through the weights and dpos
-                    R Q2[3];
-#pragma unroll
-                    for (int i = 0; i < 3; ++i)
-                        Q2[i] = pm * (v[i] + C[3 * i] * dp[0] + C[3 * i + 1] * dp[1] + C[3 * i + 2] * dp[2])
-                              + (sk[3 * i] * dp[0] + sk[3 * i + 1] * dp[1] + sk[3 * i + 2] * dp[2]) * dt;
-                    R mq = mb[0] * Q2[0] + mb[1] * Q2[1] + mb[2] * Q2[2] + gb[0] * pm;
-#pragma unroll
-                    for (int i = 0; i < 3; ++i)
-                        xb[i] += mq * dW[i]
-                               - (pm * (C[i] * mb[0] + C[3 + i] * mb[1] + C[6 + i] * mb[2])
-                                  + dt * (sk[i] * mb[0] + sk[3 + i] * mb[1] + sk[6 + i] * mb[2])) * wt;
-                }
-                const R wp = wt * pm;
-#pragma unroll
-                for (int i = 0; i < 3; ++i) {
-                    vb[i] += wp * mb[i];
-#pragma unroll
-                    for (int j = 0; j < 3; ++j) Sb[3 * i + j] += wt * (mb[i] * dp[j]);
-                }
-            }
-    R Cb[9], skb[9], taub[9];
+    for (int i = 0; i < 3; ++i) vb[i] = pm * wmb[i];
 #pragma unroll
     for (int i = 0; i < 9; ++i) {
         Cb[i] = pm * Sb[i];
@@ -700,13 +831,7 @@ bwd_particle_kernel(Ctx ctx, Tape<R> tp, const R* __restrict__ gridb, MpmParticl
     }
     if (dA) dA[sidx] = (sc.growth_mode == 1) ? (Fgl[0] + Fgl[4] + Fgl[8]) * (double)gphi : 0.0;
     if (!finite9(Fb) || !finite9(Cb)) raise_status(ctx.status, MPM_ERR_NONFINITE);
-    unsigned k = tp.skeys[sidx];
-    if (sidx == 0 || tp.skeys[sidx - 1] != k) {
-        if ((long long)k - ax.cell_begin < ax.ncells) {
-            ctx.cell_first[k] = 0;
-            ctx.cell_last[k] = 0;
-        }
-    }
+    unmark_cell(ctx, ax, tp.skeys, sidx);
 }
 
 // ---------------------------------------------------------------------------

@@ -39,7 +39,8 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--scenes", type=int, default=256)
     ap.add_argument("--mpm-steps", type=int, default=200)
-    ap.add_argument("--ckpt-every", type=int, default=0, help="0 = sqrt(N) schedule")
+    ap.add_argument("--ckpt-every", default="auto",
+                    help="checkpoint interval: an int, 'sqrt', or 'auto' (largest that fits 75%% of free HBM)")
     ap.add_argument("--no-plain", action="store_true", help="skip the FP64 plain-path leg")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
@@ -219,10 +220,12 @@ def main():
 
     scn = S.config4(seed=4 + 1000 * rank, n_scenes=a.scenes)
     n_tot = sum(s["x"].shape[0] for s in scn)
-    k = a.ckpt_every or sqrt_schedule(a.mpm_steps)
+    ck = a.ckpt_every if a.ckpt_every in ("auto", "sqrt") else int(a.ckpt_every)
     tuning = load_tuned(scn, torch.float32) or {}
-    b = Batch(scn, a.mpm_steps, dtype=torch.float32, ckpt_every=k, tuning=tuning)
-    slab_h = torch.from_numpy(host_slab(scn, np.float32)).pin_memory()
+    slab_np = host_slab(scn, np.float32)
+    b = Batch(scn, a.mpm_steps, dtype=torch.float32, ckpt_every=ck, tuning=tuning, slab_host=slab_np)
+    k = b.ckpt_every
+    slab_h = torch.from_numpy(slab_np).pin_memory()
     b.load(slab_h, non_blocking=False)
     plan = b.plan
 
@@ -316,6 +319,7 @@ def main():
     step_roof = {"bytes_per_particle_step": w * (156 + 32 * 0.2), "achieved_gbs": step_bytes / (ms_per / 1e3) / 1e9,
                  "frac": step_bytes / (ms_per / 1e3) / 1e9 / peak}
     fallbacks = plan.fp64_fallbacks()
+    status = plan.status()
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
             "ms_per_step": ms_per, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -327,7 +331,8 @@ def main():
             "roofline": roof, "step_roofline": step_roof, "e2e": e2e,
             "gpu_launches": int(launches_per_traj * a.steps), "clocks": clk,
             "kernel_ms_per_trajectory": {kk: round(v[0], 3) for kk, v in prof_all.items()},
-            "fp64_hencky_fallbacks_per_trajectory": None}
+            "fp64_hencky_fallbacks_per_trajectory": None, "device_status": status,
+            "active_tile_cap": plan.tuning.get("active_tile_cap")}
     line["fp64_hencky_fallbacks_per_trajectory"] = fallbacks / max(1, a.warmup + a.steps + 3)
 
     if rank == 0 and not a.no_plain:
@@ -354,7 +359,7 @@ def plain_leg(scn, a, value32):
     errs = {"F": 0.0, "x": 0.0, "dLdg_rel": 0.0}
     for i in sample:
         s = scn[i]
-        b64 = Batch([s], a.mpm_steps, dtype=torch.float64, ckpt_every=a.ckpt_every or None)
+        b64 = Batch([s], a.mpm_steps, dtype=torch.float64, ckpt_every="auto")
         b64.load(host_slab([s], np.float64), non_blocking=False)
         b64.run()                                     # warm-up
         torch.cuda.synchronize()
@@ -363,7 +368,7 @@ def plain_leg(scn, a, value32):
         torch.cuda.synchronize()
         secs += time.perf_counter() - t0
         units += s["x"].shape[0] * a.mpm_steps
-        b32 = Batch([s], a.mpm_steps, dtype=torch.float32, ckpt_every=a.ckpt_every or None)
+        b32 = Batch([s], a.mpm_steps, dtype=torch.float32, ckpt_every="auto")
         b32.load(host_slab([s], np.float32), non_blocking=False)
         b32.run()
         torch.cuda.synchronize()

@@ -129,6 +129,10 @@ int mpm_plan_read_fp64_fallbacks(MpmPlan* plan, int64_t* count, void* stream);
  * replay. */
 int mpm_plan_profile_begin(MpmPlan* plan, uint32_t kind_mask, int32_t max_launches);
 int mpm_plan_profile_end(MpmPlan* plan, double* ms_per_kind, int32_t* launches_per_kind);
+/* Number of active node tiles recorded in a tape (NULL: the workspace's own
+ * scratch tape of the last untaped step).  Synchronises the stream. */
+int mpm_plan_active_tiles(MpmPlan* plan, const void* tape, int32_t* n_active, void* stream);
+
 /* Kernel launches issued by this plan so far (host-side count; a captured
  * graph's launches are counted once, at capture). */
 int64_t mpm_plan_launch_count(const MpmPlan* plan);

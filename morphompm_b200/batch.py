@@ -24,7 +24,7 @@ import torch
 
 from . import _lib as L
 from .runtime import Plan, SceneSpec, SLAB_ROWS, ROW_F, ROW_X
-from .trajectory import Rollout
+from .trajectory import Rollout, budget_schedule, sqrt_schedule
 
 MODEL_KIND = {"nh": L.MODEL_NEOHOOKEAN, "hencky": L.MODEL_HENCKY, "hb": L.MODEL_HERSCHEL_BULKLEY}
 
@@ -66,27 +66,67 @@ class Batch:
     """A batch of scenes with a graph-captured forward+adjoint trajectory."""
 
     def __init__(self, scenes: List[dict], n_steps: int, dtype=torch.float32, advect: bool = True,
-                 ckpt_every: Optional[int] = None, tuning: Optional[dict] = None, loss: str = "detF",
-                 x_obs: Optional[np.ndarray] = None, device=None):
+                 ckpt_every=None, tuning: Optional[dict] = None, loss: str = "detF",
+                 x_obs: Optional[np.ndarray] = None, device=None, active_cap="auto",
+                 memory_fraction: float = 0.75, slab_host: Optional[np.ndarray] = None):
+        """ckpt_every: int, None (store every step), "sqrt", or "auto" (largest
+        interval that fits memory_fraction of the free device memory).
+        active_cap: "auto" sizes the tapes' active-tile lists from a probe
+        forward run of slab_host (1.25x its maximum), None keeps every tile."""
         self.scenes = scenes
         self.n_steps = n_steps
         self.dtype = dtype
         self.specs = [scene_spec_from_dict(s) for s in scenes]
         self.n = sum(sp.n for sp in self.specs)
-        self.plan = Plan(self.specs, dtype=dtype, tuning=tuning, device=device)
         npd = np.float32 if dtype == torch.float32 else np.float64
+        tuning = dict(tuning or {})
         phi = host_phi(scenes, npd)
-        self.phi = None
-        if phi is not None:
-            self.phi = torch.as_tensor(phi).to(self.plan.device)
-            self.plan.set_growth_field(self.phi)
+        if active_cap == "auto":
+            probe = Plan(self.specs, dtype=dtype, tuning=tuning, device=device)
+            self._set_phi(probe, phi)
+            tuning["active_tile_cap"] = self._probe_active(probe, slab_host if slab_host is not None
+                                                           else host_slab(scenes, npd), advect)
+            del probe
+        elif active_cap:
+            tuning["active_tile_cap"] = int(active_cap)
+        self.plan = Plan(self.specs, dtype=dtype, tuning=tuning, device=device)
+        self.phi = self._set_phi(self.plan, phi)
+        state_bytes = SLAB_ROWS * self.n * self.plan.real_bytes
+        if ckpt_every == "sqrt":
+            ckpt_every = sqrt_schedule(n_steps)
+        elif ckpt_every == "auto":
+            free, _ = torch.cuda.mem_get_info(self.plan.device)
+            ckpt_every = budget_schedule(n_steps, state_bytes, self.plan.tape_bytes, int(memory_fraction * free))
+        self.ckpt_every = ckpt_every or n_steps
         xo = None
         if loss == "mse":
             xo = torch.as_tensor(np.ascontiguousarray(x_obs.T.astype(npd))).to(self.plan.device)
-        self.rollout = Rollout(self.plan, n_steps, advect=advect, ckpt_every=ckpt_every, Fg=None, loss=loss,
+        self.rollout = Rollout(self.plan, n_steps, advect=advect, ckpt_every=self.ckpt_every, Fg=None, loss=loss,
                                x_obs=xo)
         self.slab0 = torch.empty(SLAB_ROWS, self.n, dtype=dtype, device=self.plan.device)
         self.graph = None
+
+    @staticmethod
+    def _set_phi(plan, phi):
+        if phi is None:
+            return None
+        t = torch.as_tensor(phi).to(plan.device)
+        plan.set_growth_field(t)
+        return t
+
+    def _probe_active(self, plan, slab_host, advect) -> int:
+        """Run the forward trajectory once without tapes and return a tape
+        capacity of 1.25x the largest active-tile count seen (+16)."""
+        from .runtime import slab_particles
+        dev = plan.device
+        a = torch.as_tensor(slab_host).to(dev)
+        b = torch.empty_like(a)
+        mx = 0
+        for t in range(self.n_steps):
+            plan.step_fwd(slab_particles(a), slab_particles(b), advect, t, None)
+            mx = max(mx, plan.active_tiles(None))
+            a, b = b, a
+        return int(1.25 * mx) + 16
 
     def particle_steps(self) -> int:
         return self.n * self.n_steps
@@ -160,7 +200,7 @@ def autotune(scenes: List[dict], dtype=torch.float32, steps: int = 4, budget_s: 
     slab = torch.as_tensor(host_slab(scenes, np.float32 if dtype == torch.float32 else np.float64))
 
     def measure(cfg):
-        b = Batch(scenes, steps, dtype=dtype, tuning=cfg, ckpt_every=steps)
+        b = Batch(scenes, steps, dtype=dtype, tuning=cfg, ckpt_every=steps, active_cap=None)
         b.load(slab.to(b.plan.device), non_blocking=False)
         ro = b.rollout
         ro.forward(b.slab0)

@@ -440,6 +440,14 @@ int mpm_plan_profile_end(MpmPlan* P, double* ms_per_kind, int32_t* launches_per_
 
 int64_t mpm_plan_launch_count(const MpmPlan* P) { return P ? P->launches : -1; }
 
+int mpm_plan_active_tiles(MpmPlan* P, const void* tape, int32_t* n_active, void* stream) {
+    if (!P || !P->ws || !n_active) return MPM_ERR_ARG;
+    const char* t = tape ? static_cast<const char*>(tape) : P->ws + P->o_tape;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (cudaMemcpyAsync(n_active, t + P->t_nact, 4, cudaMemcpyDeviceToHost, st) != cudaSuccess) return MPM_ERR_CUDA;
+    return cudaStreamSynchronize(st) == cudaSuccess ? MPM_OK : MPM_ERR_CUDA;
+}
+
 int mpm_plan_workspace_bytes(const MpmPlan* P, size_t* bytes) {
     if (!P || !bytes) return MPM_ERR_ARG;
     *bytes = P->ws_bytes;

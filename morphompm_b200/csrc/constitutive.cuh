@@ -20,10 +20,17 @@ namespace mpm {
 // On return lam[i] are the eigenvalues and column i of V (row-major) the
 // corresponding unit eigenvector.
 // ---------------------------------------------------------------------------
+// One rotation annihilating A[p][q].  An off-diagonal entry at or below the
+// rounding level of its diagonal (|a_pq| <= eps (|a_pp| + |a_qq|) / 4) is set to
+// zero without rotating; returns whether a rotation was applied.
 template <typename R>
-__device__ __forceinline__ void jacobi_rotate(R A[3][3], R V[9], int p, int q) {
+__device__ __forceinline__ bool jacobi_rotate(R A[3][3], R V[9], int p, int q) {
     R apq = A[p][q];
-    if (apq == R(0)) return;
+    if (d_abs(apq) <= R(0.25) * Num<R>::eps * (d_abs(A[p][p]) + d_abs(A[q][q]))) {
+        A[p][q] = R(0);
+        A[q][p] = R(0);
+        return false;
+    }
     R theta = (A[q][q] - A[p][p]) / (R(2) * apq);
     R t = R(1) / (d_abs(theta) + d_sqrt(theta * theta + R(1)));
     if (theta < R(0)) t = -t;
@@ -46,8 +53,11 @@ __device__ __forceinline__ void jacobi_rotate(R A[3][3], R V[9], int p, int q) {
         V[3 * k + p] = vkp - s * (vkq + tau * vkp);
         V[3 * k + q] = vkq + s * (vkp - tau * vkq);
     }
+    return true;
 }
 
+// Cyclic sweeps until a sweep finds every off-diagonal entry at rounding level
+// (quadratic convergence: typically 3-4 sweeps in FP64, 2-3 in FP32).
 template <typename R>
 __device__ __forceinline__ void sym_eig3(const R S[9], R lam[3], R V[9]) {
     R A[3][3];
@@ -57,15 +67,12 @@ __device__ __forceinline__ void sym_eig3(const R S[9], R lam[3], R V[9]) {
         for (int j = 0; j < 3; ++j) A[i][j] = R(0.5) * (S[3 * i + j] + S[3 * j + i]);
 #pragma unroll
     for (int i = 0; i < 9; ++i) V[i] = (i % 4 == 0) ? R(1) : R(0);
-    const int max_sweeps = sizeof(R) == 8 ? 12 : 8;
-    const R tol = Num<R>::eps * Num<R>::eps;
+    const int max_sweeps = sizeof(R) == 8 ? 10 : 6;
     for (int sweep = 0; sweep < max_sweeps; ++sweep) {
-        R off = A[0][1] * A[0][1] + A[0][2] * A[0][2] + A[1][2] * A[1][2];
-        R dia = A[0][0] * A[0][0] + A[1][1] * A[1][1] + A[2][2] * A[2][2];
-        if (off <= tol * dia) break;
-        jacobi_rotate(A, V, 0, 1);
-        jacobi_rotate(A, V, 0, 2);
-        jacobi_rotate(A, V, 1, 2);
+        bool r0 = jacobi_rotate(A, V, 0, 1);
+        bool r1 = jacobi_rotate(A, V, 0, 2);
+        bool r2 = jacobi_rotate(A, V, 1, 2);
+        if (!(r0 || r1 || r2)) break;
     }
     lam[0] = A[0][0];
     lam[1] = A[1][1];
@@ -349,22 +356,44 @@ __device__ __forceinline__ void hb_vjp(const R F[9], const R Fg[9], const R C[9]
 
 // ---------------------------------------------------------------------------
 // model dispatch.  Returns true when an FP32 Hencky evaluation went to FP64.
+// Hencky and Herschel-Bulkley are called out of line so that their register
+// demand (the eigensolve, the FP64 recompute) does not inflate the register
+// allocation of the kernels that fuse them.
 // ---------------------------------------------------------------------------
+template <typename R>
+__device__ __noinline__ bool hencky_stress_ool(const R* F, const R* Fg, R mu, R lam, float thresh, R* tau) {
+    return Hencky<R>::stress(F, Fg, mu, lam, thresh, tau);
+}
+template <typename R>
+__device__ __noinline__ bool hencky_vjp_ool(const R* F, const R* Fg, R mu, R lam, float thresh, const R* tb, R* Fb,
+                                            R* Fgb) {
+    return Hencky<R>::vjp(F, Fg, mu, lam, thresh, tb, Fb, Fgb);
+}
+template <typename R>
+__device__ __noinline__ void hb_stress_ool(const R* F, const R* Fg, const R* C, const ModelParams<R> P, R* tau) {
+    hb_stress(F, Fg, C, P, tau);
+}
+template <typename R>
+__device__ __noinline__ void hb_vjp_ool(const R* F, const R* Fg, const R* C, const ModelParams<R> P, const R* tb,
+                                        R* Fb, R* Fgb, R* Cb) {
+    hb_vjp(F, Fg, C, P, tb, Fb, Fgb, Cb);
+}
+
 template <typename R>
 __device__ __forceinline__ bool model_stress(const ModelParams<R>& P, float thresh, const R F[9], const R Fg[9],
                                              const R C[9], R tau[9]) {
-    if (P.kind == MPM_MODEL_HENCKY) return Hencky<R>::stress(F, Fg, P.mu, P.lam, thresh, tau);
-    if (P.kind == MPM_MODEL_HERSCHEL_BULKLEY) { hb_stress(F, Fg, C, P, tau); return false; }
+    if (P.kind == MPM_MODEL_HENCKY) return hencky_stress_ool<R>(F, Fg, P.mu, P.lam, thresh, tau);
+    if (P.kind == MPM_MODEL_HERSCHEL_BULKLEY) { hb_stress_ool<R>(F, Fg, C, P, tau); return false; }
     nh_stress(F, Fg, P.mu, P.lam, tau);
     return false;
 }
 template <typename R>
 __device__ __forceinline__ bool model_vjp(const ModelParams<R>& P, float thresh, const R F[9], const R Fg[9],
                                           const R C[9], const R tb[9], R Fb[9], R Fgb[9], R Cb[9]) {
-    if (P.kind == MPM_MODEL_HERSCHEL_BULKLEY) { hb_vjp(F, Fg, C, P, tb, Fb, Fgb, Cb); return false; }
+    if (P.kind == MPM_MODEL_HERSCHEL_BULKLEY) { hb_vjp_ool<R>(F, Fg, C, P, tb, Fb, Fgb, Cb); return false; }
 #pragma unroll
     for (int i = 0; i < 9; ++i) Cb[i] = R(0);
-    if (P.kind == MPM_MODEL_HENCKY) return Hencky<R>::vjp(F, Fg, P.mu, P.lam, thresh, tb, Fb, Fgb);
+    if (P.kind == MPM_MODEL_HENCKY) return hencky_vjp_ool<R>(F, Fg, P.mu, P.lam, thresh, tb, Fb, Fgb);
     nh_vjp(F, Fg, P.mu, P.lam, tb, Fb, Fgb);
     return false;
 }

@@ -590,7 +590,8 @@ g2p_kernel(Ctx ctx, Tape<R> tp, MpmParticles in, MpmParticles out, int advect) {
     bspline(fx, w);
     Stencil<T> st;
     st.init(ctx, sc, ax, tp.tile_slot, base);
-    R nv[3] = {0, 0, 0}, nC[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    // nC = k4 sum w g (o - fx)^T dx = k4 dx (G - nv fx^T),  G[i][d] = sum w g_i o_d
+    R nv[3] = {0, 0, 0}, G[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
 #pragma unroll
     for (int a = 0; a < 3; ++a)
 #pragma unroll
@@ -602,15 +603,21 @@ g2p_kernel(Ctx ctx, Tape<R> tp, MpmParticles in, MpmParticles out, int advect) {
                 R g[4];
                 load_node(tp.grid, r, g);
                 const R wt = w[a][0] * w[b][1] * w[c][2];
-                const R dp[3] = {(R(a) - fx[0]) * dx, (R(b) - fx[1]) * dx, (R(c) - fx[2]) * dx};
-                const R kw = k4 * wt;
 #pragma unroll
                 for (int i = 0; i < 3; ++i) {
-                    nv[i] += wt * g[1 + i];
-#pragma unroll
-                    for (int j = 0; j < 3; ++j) nC[3 * i + j] += kw * (g[1 + i] * dp[j]);
+                    const R wg = wt * g[1 + i];
+                    nv[i] += wg;
+                    if (a) G[3 * i + 0] += R(a) * wg;
+                    if (b) G[3 * i + 1] += R(b) * wg;
+                    if (c) G[3 * i + 2] += R(c) * wg;
                 }
             }
+    R nC[9];
+    const R kd = k4 * dx;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int d = 0; d < 3; ++d) nC[3 * i + d] = kd * (G[3 * i + d] - nv[i] * fx[d]);
     R F[9];
     ld9<R>(in.F, p, in.sp9, in.sc9, F);
     R xn[3];
@@ -678,7 +685,7 @@ bwd_payload_kernel(Ctx ctx, const unsigned* __restrict__ perm, MpmParticles in, 
 // summed once per particle: x_b -= M1 sum(w gv) + M2 sum(w mb).
 // ---------------------------------------------------------------------------
 template <typename R, int T>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, sizeof(R) == 4 ? 2 : 1)
 bwd_particle_kernel(Ctx ctx, Tape<R> tp, const R* __restrict__ gridb, MpmParticles in, const R* __restrict__ outC,
                     MpmCotangents ob, MpmCotangents ib, double* __restrict__ dA, int advect, int t) {
     long long sidx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -734,9 +741,10 @@ bwd_particle_kernel(Ctx ctx, Tape<R> tp, const R* __restrict__ gridb, MpmParticl
     Stencil<T> st;
     st.init(ctx, sc, ax, tp.tile_slot, base);
 
-    R xb[3] = {0, 0, 0}, wgv[3] = {0, 0, 0}, wmb[3] = {0, 0, 0}, Sb[9];
+    // Sb = sum w mb (o - fx)^T dx = dx (GB - wmb fx^T),  GB[i][d] = sum w mb_i o_d
+    R xb[3] = {0, 0, 0}, wgv[3] = {0, 0, 0}, wmb[3] = {0, 0, 0}, GB[9];
 #pragma unroll
-    for (int i = 0; i < 9; ++i) Sb[i] = R(0);
+    for (int i = 0; i < 9; ++i) GB[i] = R(0);
 #pragma unroll
     for (int a = 0; a < 3; ++a)
 #pragma unroll
@@ -748,20 +756,20 @@ bwd_particle_kernel(Ctx ctx, Tape<R> tp, const R* __restrict__ gridb, MpmParticl
                 R gf[4], gb[4];
                 load_node(tp.grid, r, gf);
                 load_node(gridb, r, gb);
-                const R wa = a == 0 ? w[0][0] : (a == 1 ? w[1][0] : w[2][0]);
-                const R da = a == 0 ? dw[0][0] : (a == 1 ? dw[1][0] : dw[2][0]);
-                const R wt = wa * w[b][1] * w[cc][2];
-                const R dp[3] = {(R(a) - fx[0]) * dx, (R(b) - fx[1]) * dx, (R(cc) - fx[2]) * dx};
+                const R wt = w[a][0] * w[b][1] * w[cc][2];
                 const R* gv = gf + 1;
                 const R* mb = gb + 1;
 #pragma unroll
                 for (int i = 0; i < 3; ++i) {
                     wgv[i] += wt * gv[i];
-                    wmb[i] += wt * mb[i];
-#pragma unroll
-                    for (int j = 0; j < 3; ++j) Sb[3 * i + j] += wt * (mb[i] * dp[j]);
+                    const R wm = wt * mb[i];
+                    wmb[i] += wm;
+                    if (a) GB[3 * i + 0] += R(a) * wm;
+                    if (b) GB[3 * i + 1] += R(b) * wm;
+                    if (cc) GB[3 * i + 2] += R(cc) * wm;
                 }
                 if (advect) {
+                    const R dp[3] = {(R(a) - fx[0]) * dx, (R(b) - fx[1]) * dx, (R(cc) - fx[2]) * dx};
                     R beta[3];
 #pragma unroll
                     for (int i = 0; i < 3; ++i)
@@ -770,11 +778,20 @@ bwd_particle_kernel(Ctx ctx, Tape<R> tp, const R* __restrict__ gridb, MpmParticl
                     const R sfac = nvb[0] * gv[0] + nvb[1] * gv[1] + nvb[2] * gv[2]
                                  + mb[0] * pv[0] + mb[1] * pv[1] + mb[2] * pv[2] + gb[0] * pm
                                  + beta[0] * dp[0] + beta[1] * dp[1] + beta[2] * dp[2];
-                    xb[0] += sfac * (da * w[b][1] * w[cc][2] * inv_dx);
-                    xb[1] += sfac * (wa * dw[b][1] * w[cc][2] * inv_dx);
-                    xb[2] += sfac * (wa * w[b][1] * dw[cc][2] * inv_dx);
+                    xb[0] += sfac * (dw[a][0] * w[b][1] * w[cc][2] * inv_dx);
+                    xb[1] += sfac * (w[a][0] * dw[b][1] * w[cc][2] * inv_dx);
+                    xb[2] += sfac * (w[a][0] * w[b][1] * dw[cc][2] * inv_dx);
                 }
             }
+    R Sb[9];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int d = 0; d < 3; ++d) Sb[3 * i + d] = dx * (GB[3 * i + d] - wmb[i] * fx[d]);
+    // the constitutive VJP needs F, C, Fg again: reload rather than keep them live
+    ld9<R>(in.C, p, in.sp9, in.sc9, C);
+    ld9<R>(in.F, p, in.sp9, in.sc9, F);
+    load_Fg<R>(ctx, sc, in, p, t, Fg, &gphi);
     R Fb[9], vb[3], Cb[9], skb[9], taub[9];
     {
         R Cn[9], Fnb[9];

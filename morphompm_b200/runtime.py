@@ -185,6 +185,12 @@ class Plan:
         L.check(self.lib.mpm_plan_profile_end(self.handle, ms, cnt), "profile_end")
         return {k: (ms[i], cnt[i]) for i, k in enumerate(L.KERNELS) if cnt[i] > 0}
 
+    def active_tiles(self, tape: Optional["TapeBuf"] = None, stream=None) -> int:
+        v = C.c_int32()
+        L.check(self.lib.mpm_plan_active_tiles(self.handle, C.c_void_p(tape.ptr if tape is not None else 0),
+                                               C.byref(v), C.c_void_p(stream_ptr(stream))), "active_tiles")
+        return v.value
+
     def launch_count(self) -> int:
         return int(self.lib.mpm_plan_launch_count(self.handle))
 

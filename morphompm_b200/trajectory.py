@@ -26,6 +26,18 @@ def sqrt_schedule(n_steps: int) -> int:
     return max(1, int(math.ceil(math.sqrt(n_steps))))
 
 
+def budget_schedule(n_steps: int, state_bytes: int, tape_bytes: int, budget: int) -> int:
+    """Largest checkpoint interval k whose storage fits the byte budget:
+    ceil(N/k) checkpoints + (k+1) segment states + k tapes (k = N stores every
+    step and needs no recompute)."""
+    best = 1
+    for k in range(1, n_steps + 1):
+        need = ((n_steps + k - 1) // k + k + 1 + 5) * state_bytes + k * tape_bytes
+        if need <= budget:
+            best = k
+    return best
+
+
 class Rollout:
     """One batch (plan) rolled for n_steps with checkpoints every ``ckpt_every``.
 

@@ -30,6 +30,7 @@ extern "C" {
 #define MPM_WARN_OUTSIDE     8    /* a particle's stencil left the grid entirely     */
 #define MPM_ERR_TAPE        16    /* tape missing or recorded for another plan        */
 #define MPM_ERR_UNSUPPORTED 32    /* model kind / dtype not built                     */
+#define MPM_ERR_TOO_LARGE   64    /* scene does not fit the fixed no-allocation scratch */
 
 /* ---- constitutive model kinds (python/morphompm/constitutive.py) ---- */
 #define MPM_MODEL_NEOHOOKEAN        0   /* constitutive.py:25-39  */
@@ -184,6 +185,31 @@ int mpm_loss_detF(MpmPlan* plan, const void* F, int64_t sp9, int64_t sc9, double
                   void* F_bar, void* stream);
 int mpm_loss_mse(MpmPlan* plan, const void* x, int64_t sp3, int64_t sc3, const void* x_obs,
                  double* loss, void* x_bar, void* stream);
+
+/* Forward growth step of ONE scene that allocates nothing and needs no plan or
+ * workspace.  No counterpart in the reference.  It exists for callers that
+ * cannot call cudaMalloc: host applications (simulation plugins, real-time
+ * controllers) that own every device allocation themselves, and code paths
+ * that must not fail on an allocation in the middle of a run.  The caller
+ * passes the scene, the input state and the output buffers (same layout rules
+ * and semantics as mpm_step_fwd); every intermediate (keys, sort buffers, cell
+ * tables, stencil sums, grid) lives in one fixed device array of
+ * MPM_NOALLOC_SCRATCH_BYTES compiled into the library, which every GPU that
+ * loads the library holds until the process exits.
+ *   - A scene whose intermediates exceed that size returns MPM_ERR_TOO_LARGE
+ *     (e.g. FP64 fits about 25k particles on a 32^3 grid).
+ *   - scene->p_begin must be 0; scene->p_end is the particle count.
+ *   - The first call on a device looks the array up (cudaGetSymbolAddress)
+ *     with that device current; make that first call before any stream
+ *     capture.
+ *   - All calls share the one array: calls whose GPU work overlaps (two
+ *     streams, two host threads) race and must be serialised by the caller.
+ *     Each call clears the parts that must start at zero.
+ *   - status (may be NULL): if given, the call synchronises the stream and
+ *     stores the device status word (MPM_ERR_NONFINITE, MPM_WARN_OUTSIDE). */
+#define MPM_NOALLOC_SCRATCH_BYTES (32u << 20)
+int mpm_step_fwd_noalloc(const MpmScene* scene, int32_t real_bytes, const MpmParticles* in, MpmParticles* out,
+                         int32_t advect, int32_t step_index, int32_t* status, void* stream);
 
 int mpm_version(void);
 

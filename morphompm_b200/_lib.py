@@ -18,6 +18,7 @@ MPM_ERR_NONFINITE = 4
 MPM_WARN_OUTSIDE = 8
 MPM_ERR_TAPE = 16
 MPM_ERR_UNSUPPORTED = 32
+MPM_ERR_TOO_LARGE = 64
 
 KERNELS = ["bin", "sort", "mark", "compact", "prepass", "p2g", "g2p", "bwd_payload", "bwd_p2g",
            "bwd_particle", "reduce"]
@@ -80,6 +81,8 @@ EXPORTS = {
     "mpm_bin_keys": (i32, [C.POINTER(MpmScene), i32, i64, vp, vp, vp]),
     "mpm_loss_detF": (i32, [vp, vp, i64, i64, vp, vp, vp]),
     "mpm_loss_mse": (i32, [vp, vp, i64, i64, vp, vp, vp, vp]),
+    "mpm_step_fwd_noalloc": (i32, [C.POINTER(MpmScene), i32, C.POINTER(MpmParticles), C.POINTER(MpmParticles),
+                                   i32, i32, C.POINTER(i32), vp]),
 }
 
 _lib = None

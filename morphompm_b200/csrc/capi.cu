@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstring>
 #include <new>
 #include <vector>
@@ -618,3 +619,141 @@ int mpm_loss_mse(MpmPlan* P, const void* x, int64_t sp3, int64_t sc3, const void
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Forward step without device allocation (mpm_step_fwd_noalloc).  The whole
+// workspace of one single-scene forward step is carved out of one fixed
+// file-scope device array; the launch sequence is the same step_fwd_R that
+// mpm_step_fwd runs.
+// ---------------------------------------------------------------------------
+namespace {
+
+__device__ __align__(256) unsigned char g_noalloc_scratch[MPM_NOALLOC_SCRATCH_BYTES];
+
+constexpr int NOALLOC_MAX_DEVICES = 64;
+struct NoallocDevice {
+    std::atomic<void*> ptr{nullptr};
+    std::atomic<int> n_sm{0};
+};
+NoallocDevice g_noalloc_dev[NOALLOC_MAX_DEVICES];
+
+// Device address of the scratch array on the current device (looked up once
+// per device, with that device current).
+int noalloc_scratch(void** out, int* n_sm) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return MPM_ERR_CUDA;
+    if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) return MPM_ERR_UNSUPPORTED;
+    NoallocDevice& d = g_noalloc_dev[dev];
+    void* p = d.ptr.load();
+    if (!p) {
+        if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return MPM_ERR_CUDA;
+        int sm = 0;
+        if (cudaDeviceGetAttribute(&sm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return MPM_ERR_CUDA;
+        d.n_sm.store(sm);
+        d.ptr.store(p);
+    }
+    *out = p;
+    *n_sm = d.n_sm.load();
+    return MPM_OK;
+}
+
+// Forward-only workspace layout of one scene (the fields step_fwd_R reads),
+// on a plan object that owns no heap memory.
+bool noalloc_layout(MpmPlan& P, const MpmScene& sc, int real_bytes, SceneAux& a) {
+    P.real_bytes = real_bytes;
+    P.tune.tile_xy = 8;
+    P.tune.scatter_ctas_per_sm = 2;
+    P.tune.scatter_oxb = real_bytes == 4 ? 3 : 1;
+    P.tune.particle_block = 256;
+    P.tune.fp64_gap_thresh = 1e-4f;
+    const int T = P.tune.tile_xy;
+    P.TN = T * T * TILE_Z;
+    a.cell_begin = 0;
+    a.tile_begin = 0;
+    a.ncells = (sc.shape[0] + 2) * (sc.shape[1] + 2) * (sc.shape[2] + 2);
+    a.ntile[0] = (sc.shape[0] + T - 1) / T;
+    a.ntile[1] = (sc.shape[1] + T - 1) / T;
+    a.ntile[2] = (sc.shape[2] + TILE_Z - 1) / TILE_Z;
+    P.n = sc.p_end;
+    P.n_tiles = (long long)a.ntile[0] * a.ntile[1] * a.ntile[2];
+    P.n_keys = (long long)a.ncells + 1;
+    P.any_growth = sc.growth_mode == 1;
+    int bits = 1;
+    while ((1LL << bits) < P.n_keys) ++bits;
+    P.key_bits = bits;
+    P.passes = (bits + RADIX_BITS - 1) / RADIX_BITS;
+    P.nblk_sort = (int)((P.n + SORT_TILE - 1) / SORT_TILE);
+    P.nblk_seg = (int)((P.n + SEG_TILE - 1) / SEG_TILE);
+    P.active_cap = (int)P.n_tiles;
+    const size_t R = (size_t)real_bytes, n = (size_t)P.n, nt = (size_t)P.n_tiles;
+    Layout tl;
+    P.t_skeys = tl.take(n * 4);
+    P.t_perm = tl.take(n * 4);
+    P.t_slot = tl.take(nt * 4);
+    P.t_active = tl.take((size_t)P.active_cap * 4);
+    P.t_nact = tl.take(4);
+    P.t_grid = tl.take((size_t)P.active_cap * P.TN * 4 * R);
+    P.tape_bytes = tl.off;
+    Layout L;
+    P.o_scenes = L.take(sizeof(MpmScene));
+    P.o_aux = L.take(sizeof(SceneAux));
+    P.o_scene_of = L.take(n * 4);
+    P.o_tile_scene = L.take(nt * 4);
+    P.o_status = L.take(128);
+    P.o_cell_seg = L.take((size_t)P.n_keys * 4);
+    P.o_seg_first = L.take(n * 4);
+    P.o_seg_last = L.take(n * 4);
+    P.o_blk = L.take((size_t)P.nblk_seg * 4);
+    P.o_tile_flag = L.take(nt * 4);
+    P.o_keys = L.take(n * 4);
+    P.o_kalt0 = L.take(n * 4);
+    P.o_valt0 = L.take(n * 4);
+    P.o_kalt1 = L.take(n * 4);
+    P.o_valt1 = L.take(n * 4);
+    P.o_hist = L.take((size_t)RADIX * P.nblk_sort * 4);
+    P.o_totals = L.take(RADIX * 4);
+    P.o_payload = L.take(n * PAYLOAD * R);
+    P.o_sums = L.take(27 * n * 4 * R);
+    P.o_tape = L.take(P.tape_bytes);
+    P.ws_bytes = L.off;
+    return P.ws_bytes <= (size_t)MPM_NOALLOC_SCRATCH_BYTES;
+}
+
+}  // namespace
+
+extern "C" int mpm_step_fwd_noalloc(const MpmScene* scene, int32_t real_bytes, const MpmParticles* in,
+                                    MpmParticles* out, int32_t advect, int32_t step_index, int32_t* status,
+                                    void* stream) {
+    if (!scene || !in || !out || (real_bytes != 4 && real_bytes != 8)) return MPM_ERR_ARG;
+    if (!scene_ok(*scene) || scene->p_begin != 0 || scene->p_end < 1 || scene->p_end >= (1LL << 31))
+        return MPM_ERR_ARG;
+    if (!in->x || !in->v || !in->C || !in->F || !out->x || !out->v || !out->C || !out->F || in->x == out->x ||
+        in->F == out->F || (scene->growth_mode == 0 && !in->Fg))
+        return MPM_ERR_ARG;
+    MpmPlan P;                 // owns no heap memory: its vectors stay empty
+    SceneAux aux;
+    if (!noalloc_layout(P, *scene, real_bytes, aux)) return MPM_ERR_TOO_LARGE;
+    void* ws = nullptr;
+    int rc = noalloc_scratch(&ws, &P.n_sm);
+    if (rc) return rc;
+    P.ws = static_cast<char*>(ws);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    // the scene tables, and everything the step expects to start at zero
+    if (cudaMemcpyAsync(P.ws + P.o_scenes, scene, sizeof(MpmScene), cudaMemcpyHostToDevice, st) != cudaSuccess ||
+        cudaMemcpyAsync(P.ws + P.o_aux, &aux, sizeof(SceneAux), cudaMemcpyHostToDevice, st) != cudaSuccess ||
+        cudaMemsetAsync(P.ws + P.o_scene_of, 0, (size_t)P.n * 4, st) != cudaSuccess ||
+        cudaMemsetAsync(P.ws + P.o_tile_scene, 0, (size_t)P.n_tiles * 4, st) != cudaSuccess ||
+        cudaMemsetAsync(P.ws + P.o_status, 0, 128, st) != cudaSuccess ||
+        cudaMemsetAsync(P.ws + P.o_cell_seg, 0, (size_t)P.n_keys * 4, st) != cudaSuccess ||
+        cudaMemsetAsync(P.ws + P.o_tile_flag, 0, (size_t)P.n_tiles * 4, st) != cudaSuccess)
+        return MPM_ERR_CUDA;
+    rc = real_bytes == 4 ? step_fwd_R<float>(&P, *in, *out, advect, step_index, P.ws + P.o_tape, st)
+                         : step_fwd_R<double>(&P, *in, *out, advect, step_index, P.ws + P.o_tape, st);
+    if (rc) return rc;
+    if (status) {
+        if (cudaMemcpyAsync(status, P.ws + P.o_status, 4, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+            cudaStreamSynchronize(st) != cudaSuccess)
+            return MPM_ERR_CUDA;
+    }
+    return MPM_OK;
+}

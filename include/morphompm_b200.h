@@ -95,7 +95,7 @@ typedef struct MpmCotangents {
 /* Schedule knobs (picked by the autotuner; zeros select the defaults). */
 typedef struct MpmTuning {
     int32_t tile_xy;             /* node tile edge in x and y: 4, 8 or 16 (z is fixed at 14) */
-    int32_t scatter_ctas_per_sm; /* persistent P2G grid = SMs x this (default 2)            */
+    int32_t scatter_ctas_per_sm; /* persistent P2G node-gather grid = SMs x this (default 4) */
     int32_t scatter_oxb;         /* stencil x-offsets per pass: 3 (FP32 default) or 1       */
     int32_t particle_block;      /* threads per block of the per-particle kernels (256)     */
     int32_t active_tile_cap;     /* capacity of the active-tile list (0 = every tile)       */

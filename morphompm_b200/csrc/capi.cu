@@ -318,7 +318,7 @@ int mpm_plan_create(const MpmScene* scenes, int32_t n_scenes, int32_t real_bytes
     P->real_bytes = real_bytes;
     if (tuning) P->tune = *tuning;
     if (P->tune.tile_xy != 4 && P->tune.tile_xy != 16) P->tune.tile_xy = 8;
-    if (P->tune.scatter_ctas_per_sm <= 0) P->tune.scatter_ctas_per_sm = 2;
+    if (P->tune.scatter_ctas_per_sm <= 0) P->tune.scatter_ctas_per_sm = 4;
     if (P->tune.scatter_oxb != 1 && P->tune.scatter_oxb != 3) P->tune.scatter_oxb = real_bytes == 4 ? 3 : 1;
     if (real_bytes == 8) P->tune.scatter_oxb = 1;
     if (P->tune.particle_block <= 0 || P->tune.particle_block > 1024 || P->tune.particle_block % 32)

@@ -355,6 +355,46 @@ __device__ __forceinline__ void hb_vjp(const R F[9], const R Fg[9], const R C[9]
 }
 
 // ---------------------------------------------------------------------------
+// Hencky with the eigendecomposition kept between the stress (before the P2G
+// adjoint gather) and the VJP (after it): one eigensolve per particle in the
+// reverse kernel.  keep = {beta[3], V[9], flag}; flag 1 means the FP32 stress
+// went to FP64 and the VJP must do the same.
+// ---------------------------------------------------------------------------
+template <typename R>
+__device__ __noinline__ bool hencky_stress_keep(const R* F, const R* Fg, R mu, R lam, float thresh, R* tau,
+                                                R* keep) {
+    R Fgi[9], Fe[9], beta[3], V[9];
+    hencky_eig(F, Fg, Fgi, Fe, beta, V);
+    bool fp64 = false;
+    if constexpr (sizeof(R) == 4) fp64 = sv_gap(beta) < thresh;
+    if (fp64) {
+        Hencky<R>::stress(F, Fg, mu, lam, thresh, tau);
+    } else {
+        hencky_tau_from_eig(beta, V, mu, lam, tau);
+    }
+#pragma unroll
+    for (int i = 0; i < 3; ++i) keep[i] = beta[i];
+#pragma unroll
+    for (int i = 0; i < 9; ++i) keep[3 + i] = V[i];
+    keep[12] = fp64 ? R(1) : R(0);
+    return fp64;
+}
+template <typename R>
+__device__ __noinline__ bool hencky_vjp_keep(const R* F, const R* Fg, R mu, R lam, float thresh, const R* tb,
+                                             const R* keep, R* Fb, R* Fgb) {
+    if (keep[12] != R(0)) return Hencky<R>::vjp(F, Fg, mu, lam, thresh, tb, Fb, Fgb);
+    R Fgi[9], Fe[9], beta[3], V[9];
+    inv3(Fg, Fgi);
+    mm(F, Fgi, Fe);
+#pragma unroll
+    for (int i = 0; i < 3; ++i) beta[i] = keep[i];
+#pragma unroll
+    for (int i = 0; i < 9; ++i) V[i] = keep[3 + i];
+    hencky_vjp_from_eig(F, Fgi, Fe, beta, V, mu, lam, tb, Fb, Fgb);
+    return false;
+}
+
+// ---------------------------------------------------------------------------
 // model dispatch.  Returns true when an FP32 Hencky evaluation went to FP64.
 // Hencky and Herschel-Bulkley are called out of line so that their register
 // demand (the eigensolve, the FP64 recompute) does not inflate the register
@@ -396,6 +436,25 @@ __device__ __forceinline__ bool model_vjp(const ModelParams<R>& P, float thresh,
     if (P.kind == MPM_MODEL_HENCKY) return hencky_vjp_ool<R>(F, Fg, P.mu, P.lam, thresh, tb, Fb, Fgb);
     nh_vjp(F, Fg, P.mu, P.lam, tb, Fb, Fgb);
     return false;
+}
+
+// Stress and VJP for the reverse kernel, sharing Hencky's eigendecomposition.
+template <typename R>
+__device__ __forceinline__ bool model_stress_keep(const ModelParams<R>& P, float thresh, const R F[9],
+                                                  const R Fg[9], const R C[9], R tau[9], R keep[13]) {
+    if (P.kind == MPM_MODEL_HENCKY) return hencky_stress_keep<R>(F, Fg, P.mu, P.lam, thresh, tau, keep);
+    return model_stress(P, thresh, F, Fg, C, tau);
+}
+template <typename R>
+__device__ __forceinline__ bool model_vjp_keep(const ModelParams<R>& P, float thresh, const R F[9], const R Fg[9],
+                                               const R C[9], const R tb[9], const R keep[13], R Fb[9], R Fgb[9],
+                                               R Cb[9]) {
+    if (P.kind == MPM_MODEL_HENCKY) {
+#pragma unroll
+        for (int i = 0; i < 9; ++i) Cb[i] = R(0);
+        return hencky_vjp_keep<R>(F, Fg, P.mu, P.lam, thresh, tb, keep, Fb, Fgb);
+    }
+    return model_vjp(P, thresh, F, Fg, C, tb, Fb, Fgb, Cb);
 }
 
 }  // namespace mpm

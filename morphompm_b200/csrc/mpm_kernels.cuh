@@ -468,7 +468,6 @@ node_sums_kernel(Ctx ctx, const R* __restrict__ S, long long cap, const int* __r
             const int i = L0 + nx, j = L1 + ny, k = L2 + nz;
             if (i >= sc.shape[0] || j >= sc.shape[1] || k >= sc.shape[2]) continue;
             R acc[4] = {R(0), R(0), R(0), R(0)};
-            // source cell of offset o is padded cell (i,j,k) + 2 - o
             const long long cbase = ax.cell_begin + ((long long)(i + 2) * P1 + (j + 2)) * P2 + (k + 2);
 #pragma unroll
             for (int ox = 0; ox < 3; ++ox)
@@ -558,6 +557,24 @@ struct Stencil {
         if (sl < 0) return -1;
         return sl * (T * T * TILE_Z) + (lc[0][a] * T + lc[1][b]) * TILE_Z + lc[2][c];
     }
+    // Records of column (a,b) for the first and the second z-tile (-1 if the
+    // column is off the grid or its tile is inactive); node (a,b,c) is then
+    // (sel[2][c] ? r1 : r0) + lc[2][c] when sel[2][c] >= 0.
+    __device__ __forceinline__ void column(int a, int b, long long& r0, long long& r1) const {
+        const int x = sel[0][a], y = sel[1][b];
+        if (x < 0 || y < 0) { r0 = -1; r1 = -1; return; }
+        const long long z0 = x ? (y ? s110 : s100) : (y ? s010 : s000);
+        const long long z1 = x ? (y ? s111 : s101) : (y ? s011 : s001);
+        const long long off = (long long)(lc[0][a] * T + lc[1][b]) * TILE_Z;
+        r0 = z0 < 0 ? -1 : z0 * (T * T * TILE_Z) + off;
+        r1 = z1 < 0 ? -1 : z1 * (T * T * TILE_Z) + off;
+    }
+    __device__ __forceinline__ long long node(long long r0, long long r1, int c) const {
+        const int z = sel[2][c];
+        if (z < 0) return -1;
+        const long long r = z ? r1 : r0;
+        return r < 0 ? -1 : r + lc[2][c];
+    }
 };
 
 __device__ __forceinline__ void unmark_cell(const Ctx& ctx, const SceneAux& ax, const unsigned* __restrict__ skeys,
@@ -595,10 +612,12 @@ g2p_kernel(Ctx ctx, Tape<R> tp, MpmParticles in, MpmParticles out, int advect) {
 #pragma unroll
     for (int a = 0; a < 3; ++a)
 #pragma unroll
-        for (int b = 0; b < 3; ++b)
+        for (int b = 0; b < 3; ++b) {
+            long long r0, r1;
+            st.column(a, b, r0, r1);
 #pragma unroll
             for (int c = 0; c < 3; ++c) {
-                long long r = st.rec(a, b, c);
+                long long r = st.node(r0, r1, c);
                 if (r < 0) continue;
                 R g[4];
                 load_node(tp.grid, r, g);
@@ -612,6 +631,7 @@ g2p_kernel(Ctx ctx, Tape<R> tp, MpmParticles in, MpmParticles out, int advect) {
                     if (c) G[3 * i + 2] += R(c) * wg;
                 }
             }
+        }
     R nC[9];
     const R kd = k4 * dx;
 #pragma unroll
@@ -706,8 +726,8 @@ bwd_particle_kernel(Ctx ctx, Tape<R> tp, const R* __restrict__ gridb, MpmParticl
     ld9<R>(in.F, p, in.sp9, in.sc9, F);
     load_Fg<R>(ctx, sc, in, p, t, Fg, &gphi);
 
-    R tau[9];
-    bool fb = model_stress(M, ctx.gap_thresh, F, Fg, C, tau);
+    R tau[9], keep[13];
+    bool fb = model_stress_keep(M, ctx.gap_thresh, F, Fg, C, tau, keep);
     const R c = -k4 * (R)sc.vol0 * det3(Fg);
 
     // per-particle matrices of the regrouped x_b terms
@@ -748,10 +768,12 @@ bwd_particle_kernel(Ctx ctx, Tape<R> tp, const R* __restrict__ gridb, MpmParticl
 #pragma unroll
     for (int a = 0; a < 3; ++a)
 #pragma unroll
-        for (int b = 0; b < 3; ++b)
+        for (int b = 0; b < 3; ++b) {
+            long long r0, r1;
+            st.column(a, b, r0, r1);
 #pragma unroll
             for (int cc = 0; cc < 3; ++cc) {
-                long long r = st.rec(a, b, cc);
+                long long r = st.node(r0, r1, cc);
                 if (r < 0) continue;
                 R gf[4], gb[4];
                 load_node(tp.grid, r, gf);
@@ -783,6 +805,7 @@ bwd_particle_kernel(Ctx ctx, Tape<R> tp, const R* __restrict__ gridb, MpmParticl
                     xb[2] += sfac * (w[a][0] * w[b][1] * dw[cc][2] * inv_dx);
                 }
             }
+        }
     R Sb[9];
 #pragma unroll
     for (int i = 0; i < 3; ++i)
@@ -819,7 +842,7 @@ bwd_particle_kernel(Ctx ctx, Tape<R> tp, const R* __restrict__ gridb, MpmParticl
         taub[i] = c * skb[i];
     }
     R Fb2[9], Fgb[9], Cb2[9];
-    fb |= model_vjp(M, ctx.gap_thresh, F, Fg, C, taub, Fb2, Fgb, Cb2);
+    fb |= model_vjp_keep(M, ctx.gap_thresh, F, Fg, C, taub, keep, Fb2, Fgb, Cb2);
     if (fb) atomicAdd(ctx.fallbacks, 1ull);
 #pragma unroll
     for (int i = 0; i < 9; ++i) {

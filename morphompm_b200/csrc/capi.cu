@@ -46,7 +46,9 @@ struct MpmPlan {
     bool any_growth = false;
     // workspace offsets
     size_t o_scenes, o_aux, o_scene_of, o_tile_scene, o_status, o_cell_seg, o_seg_first, o_seg_last, o_blk;
-    size_t o_tile_flag, o_keys, o_kalt0, o_valt0, o_kalt1, o_valt1, o_hist, o_totals, o_payload, o_sums, o_gridb;
+    size_t o_tile_flag, o_keys, o_kalt0, o_valt0, o_kalt1, o_valt1, o_hist, o_totals, o_payload, o_sums;
+    size_t o_dense_f = 0, o_dense_b = 0;
+    long long n_nodes = 0;
     size_t o_dbuf, o_tape;
     int nblk_seg = 1;
     size_t ws_bytes = 0;
@@ -83,6 +85,8 @@ Ctx make_ctx(MpmPlan* P) {
     c.blk_count = at<unsigned>(P, P->o_blk);
     c.tile_flag = at<int>(P, P->o_tile_flag);
     c.phi = P->phi;
+    c.dense_f = P->ws + P->o_dense_f;
+    c.dense_b = P->ws + P->o_dense_b;
     c.n = P->n;
     c.n_tiles = P->n_tiles;
     c.n_scenes = (int)P->scenes.size();
@@ -248,7 +252,6 @@ int step_bwd_T(MpmPlan* P, const MpmParticles& in, const void* outC, const MpmCo
     const int B = P->tune.particle_block;
     const int g = grid_for(P->n, B);
     R* payload = at<R>(P, P->o_payload);
-    R* gridb = at<R>(P, P->o_gridb);
     double* dbuf = at<double>(P, P->o_dbuf);
     int rc = build_segments(P, ctx, tp.skeys, 0, st);
     if (rc) return rc;
@@ -260,13 +263,13 @@ int step_bwd_T(MpmPlan* P, const MpmParticles& in, const void* outC, const MpmCo
     if (rc) return rc;
     {
         Site s(P, MPM_K_BWD_P2G, 1, st);
-        rc = launch_p2g<R>(P, 1, ctx, payload, tp.active, tp.n_active, gridb, tp.grid, advect, st);
+        rc = launch_p2g<R>(P, 1, ctx, payload, tp.active, tp.n_active, nullptr, tp.grid, advect, st);
     }
     if (rc) return rc;
     bool want_dA = growth_grad != nullptr && P->any_growth;
     {
         Site s(P, MPM_K_BWD_PARTICLE, 1, st);
-        bwd_particle_kernel<R, T><<<g, B, 0, st>>>(ctx, tp, gridb, in, static_cast<const R*>(outC), ob, ib,
+        bwd_particle_kernel<R, T><<<g, B, 0, st>>>(ctx, tp, in, static_cast<const R*>(outC), ob, ib,
                                                    want_dA ? dbuf : nullptr, advect, t);
     }
     if (want_dA) {
@@ -326,7 +329,7 @@ int mpm_plan_create(const MpmScene* scenes, int32_t n_scenes, int32_t real_bytes
     if (P->tune.fp64_gap_thresh == 0.0f) P->tune.fp64_gap_thresh = 1e-4f;
     const int T = P->tune.tile_xy;
     P->TN = T * T * TILE_Z;
-    long long cell = 0, tile = 0, pcur = 0;
+    long long cell = 0, tile = 0, pcur = 0, nodes = 0;
     for (int s = 0; s < n_scenes; ++s) {
         const MpmScene& sc = scenes[s];
         if (!scene_ok(sc) || sc.p_begin != pcur) { delete P; return MPM_ERR_ARG; }
@@ -338,6 +341,8 @@ int mpm_plan_create(const MpmScene* scenes, int32_t n_scenes, int32_t real_bytes
         a.ntile[1] = (sc.shape[1] + T - 1) / T;
         a.ntile[2] = (sc.shape[2] + TILE_Z - 1) / TILE_Z;
         a.tile_begin = tile;
+        a.node_begin = nodes;
+        nodes += (long long)sc.shape[0] * sc.shape[1] * sc.shape[2];
         cell += (long long)a.ncells + 1;
         tile += (long long)a.ntile[0] * a.ntile[1] * a.ntile[2];
         P->scenes.push_back(sc);
@@ -350,6 +355,7 @@ int mpm_plan_create(const MpmScene* scenes, int32_t n_scenes, int32_t real_bytes
     P->n = pcur;
     P->n_tiles = tile;
     P->n_keys = cell;
+    P->n_nodes = nodes;
     int bits = 1;
     while ((1LL << bits) < cell) ++bits;
     P->key_bits = bits;
@@ -389,7 +395,8 @@ int mpm_plan_create(const MpmScene* scenes, int32_t n_scenes, int32_t real_bytes
     P->o_totals = L.take(RADIX * 4);
     P->o_payload = L.take(n * PAYLOAD * R);
     P->o_sums = L.take(27 * n * 4 * R);
-    P->o_gridb = L.take((size_t)P->active_cap * P->TN * 4 * R);
+    P->o_dense_f = L.take((size_t)P->n_nodes * 4 * R);
+    P->o_dense_b = L.take((size_t)P->n_nodes * 4 * R);
     P->o_dbuf = L.take(n * 8);
     P->o_tape = L.take(P->tape_bytes);
     P->ws_bytes = L.off;
@@ -670,6 +677,7 @@ bool noalloc_layout(MpmPlan& P, const MpmScene& sc, int real_bytes, SceneAux& a)
     P.TN = T * T * TILE_Z;
     a.cell_begin = 0;
     a.tile_begin = 0;
+    a.node_begin = 0;
     a.ncells = (sc.shape[0] + 2) * (sc.shape[1] + 2) * (sc.shape[2] + 2);
     a.ntile[0] = (sc.shape[0] + T - 1) / T;
     a.ntile[1] = (sc.shape[1] + T - 1) / T;
@@ -677,6 +685,7 @@ bool noalloc_layout(MpmPlan& P, const MpmScene& sc, int real_bytes, SceneAux& a)
     P.n = sc.p_end;
     P.n_tiles = (long long)a.ntile[0] * a.ntile[1] * a.ntile[2];
     P.n_keys = (long long)a.ncells + 1;
+    P.n_nodes = (long long)sc.shape[0] * sc.shape[1] * sc.shape[2];
     P.any_growth = sc.growth_mode == 1;
     int bits = 1;
     while ((1LL << bits) < P.n_keys) ++bits;
@@ -714,6 +723,8 @@ bool noalloc_layout(MpmPlan& P, const MpmScene& sc, int real_bytes, SceneAux& a)
     P.o_totals = L.take(RADIX * 4);
     P.o_payload = L.take(n * PAYLOAD * R);
     P.o_sums = L.take(27 * n * 4 * R);
+    P.o_dense_f = L.take((size_t)P.n_nodes * 4 * R);
+    P.o_dense_b = P.o_dense_f;      // the forward step writes no reverse records
     P.o_tape = L.take(P.tape_bytes);
     P.ws_bytes = L.off;
     return P.ws_bytes <= (size_t)MPM_NOALLOC_SCRATCH_BYTES;

@@ -19,6 +19,7 @@ constexpr int TILE_Z = 16;
 struct SceneAux {
     long long cell_begin;   // first padded cell key of the scene
     long long tile_begin;   // first node tile of the scene
+    long long node_begin;   // first node of the scene in the dense node scratch
     int ntile[3];           // tiles per axis
     int ncells;             // (shape+2)^3 padded cells; key cell_begin+ncells = "outside"
 };
@@ -38,6 +39,8 @@ struct Ctx {
     unsigned* blk_count;         // per-block segment counts of the segment scan
     int* tile_flag;              // 1 if the tile receives mass this step
     const void* phi;             // growth field phi_p (growth_mode 1), may be null
+    void* dense_f;               // dense node scratch, forward record (m, v[3]) per node
+    void* dense_b;               // dense node scratch, reverse record (gm_b, gmom_b[3]) per node
     long long n;
     long long n_tiles;
     int n_scenes;

@@ -483,6 +483,7 @@ node_sums_kernel(Ctx ctx, const R* __restrict__ S, long long cap, const int* __r
                         }
                     }
             const long long gidx = (long long)it * TN + node;
+            const long long didx = ax.node_begin + ((long long)i * sc.shape[1] + j) * sc.shape[2] + k;
             R rec[4] = {R(0), R(0), R(0), R(0)};
             if constexpr (MODE == 0) {
                 const R m = acc[0];
@@ -495,6 +496,7 @@ node_sums_kernel(Ctx ctx, const R* __restrict__ S, long long cap, const int* __r
             } else {
                 R f[4];
                 load_node(grid_fwd, gidx, f);
+                store_node(static_cast<R*>(ctx.dense_f), didx, f);
                 const R m = f[0];
                 if (m > eps && node_free(sc, i, j, k)) {
                     rec[1] = (s_damp * acc[0]) / m;
@@ -506,74 +508,37 @@ node_sums_kernel(Ctx ctx, const R* __restrict__ S, long long cap, const int* __r
                     }
                 }
             }
-            store_node(grid_out, gidx, rec);
+            if constexpr (MODE == 0) {
+                store_node(grid_out, gidx, rec);
+                store_node(static_cast<R*>(ctx.dense_f), didx, rec);
+            } else {
+                store_node(static_cast<R*>(ctx.dense_b), didx, rec);
+            }
         }
     }
 }
 
 // ---------------------------------------------------------------------------
-// stencil addressing into the compact per-tile grid.  A particle's 3x3x3
-// stencil spans at most 2 tiles per axis; the (up to 8) tile slots are looked
-// up once, then every node record index is slot*TN + local.
+// stencil addressing into the dense node scratch: node (i,j,k) of a scene is
+// node_begin + (i ny + j) nz + k; per particle the three axis offsets are
+// formed once and a node costs two adds.
 // ---------------------------------------------------------------------------
-template <int T>
-struct Stencil {
-    int lc[3][3];       // coordinate inside the tile, per axis and offset
-    int sel[3][3];      // 0: first tile of the axis, 1: second, -1: node off the grid
-    long long s000, s001, s010, s011, s100, s101, s110, s111;   // tile slots (-1 missing)
-    __device__ __forceinline__ void init(const Ctx& ctx, const MpmScene& sc, const SceneAux& ax,
-                                         const int* __restrict__ tile_slot, const int base[3]) {
-        const int TT[3] = {T, T, TILE_Z};
-        int t0[3], t1[3];
+struct DenseStencil {
+    long long ox[3], oy[3];
+    int oz[3];
+    bool vx[3], vy[3], vz[3];
+    __device__ __forceinline__ void init(const MpmScene& sc, const SceneAux& ax, const int base[3]) {
+        const long long ny = sc.shape[1], nz = sc.shape[2];
 #pragma unroll
-        for (int d = 0; d < 3; ++d) {
-            int lo = base[d] < 0 ? 0 : base[d];
-            t0[d] = lo / TT[d];
-            t1[d] = t0[d];
-#pragma unroll
-            for (int o = 0; o < 3; ++o) {
-                int n = base[d] + o;
-                bool ok = n >= 0 && n < sc.shape[d];
-                int t = ok ? n / TT[d] : t0[d];
-                if (ok && t != t0[d]) t1[d] = t;
-                sel[d][o] = ok ? (t == t0[d] ? 0 : 1) : -1;
-                lc[d][o] = ok ? n - t * TT[d] : 0;
-            }
+        for (int o = 0; o < 3; ++o) {
+            const int i = base[0] + o, j = base[1] + o, k = base[2] + o;
+            vx[o] = i >= 0 && i < sc.shape[0];
+            vy[o] = j >= 0 && j < sc.shape[1];
+            vz[o] = k >= 0 && k < sc.shape[2];
+            ox[o] = ax.node_begin + (long long)i * ny * nz;
+            oy[o] = (long long)j * nz;
+            oz[o] = k;
         }
-        auto look = [&](int a, int b, int c) -> long long {
-            int tx = a ? t1[0] : t0[0], ty = b ? t1[1] : t0[1], tz = c ? t1[2] : t0[2];
-            bool need = (a == 0 || t1[0] != t0[0]) && (b == 0 || t1[1] != t0[1]) && (c == 0 || t1[2] != t0[2]);
-            if (!need || tx >= ax.ntile[0] || ty >= ax.ntile[1] || tz >= ax.ntile[2]) return -1;
-            return tile_slot[ax.tile_begin + ((long long)tx * ax.ntile[1] + ty) * ax.ntile[2] + tz];
-        };
-        s000 = look(0, 0, 0); s001 = look(0, 0, 1); s010 = look(0, 1, 0); s011 = look(0, 1, 1);
-        s100 = look(1, 0, 0); s101 = look(1, 0, 1); s110 = look(1, 1, 0); s111 = look(1, 1, 1);
-    }
-    // compact record index or -1
-    __device__ __forceinline__ long long rec(int a, int b, int c) const {
-        const int x = sel[0][a], y = sel[1][b], z = sel[2][c];
-        if (x < 0 || y < 0 || z < 0) return -1;
-        long long sl = x ? (y ? (z ? s111 : s110) : (z ? s101 : s100)) : (y ? (z ? s011 : s010) : (z ? s001 : s000));
-        if (sl < 0) return -1;
-        return sl * (T * T * TILE_Z) + (lc[0][a] * T + lc[1][b]) * TILE_Z + lc[2][c];
-    }
-    // Records of column (a,b) for the first and the second z-tile (-1 if the
-    // column is off the grid or its tile is inactive); node (a,b,c) is then
-    // (sel[2][c] ? r1 : r0) + lc[2][c] when sel[2][c] >= 0.
-    __device__ __forceinline__ void column(int a, int b, long long& r0, long long& r1) const {
-        const int x = sel[0][a], y = sel[1][b];
-        if (x < 0 || y < 0) { r0 = -1; r1 = -1; return; }
-        const long long z0 = x ? (y ? s110 : s100) : (y ? s010 : s000);
-        const long long z1 = x ? (y ? s111 : s101) : (y ? s011 : s001);
-        const long long off = (long long)(lc[0][a] * T + lc[1][b]) * TILE_Z;
-        r0 = z0 < 0 ? -1 : z0 * (T * T * TILE_Z) + off;
-        r1 = z1 < 0 ? -1 : z1 * (T * T * TILE_Z) + off;
-    }
-    __device__ __forceinline__ long long node(long long r0, long long r1, int c) const {
-        const int z = sel[2][c];
-        if (z < 0) return -1;
-        const long long r = z ? r1 : r0;
-        return r < 0 ? -1 : r + lc[2][c];
     }
 };
 
@@ -605,23 +570,25 @@ g2p_kernel(Ctx ctx, Tape<R> tp, MpmParticles in, MpmParticles out, int advect) {
     bin_particle(x, inv_dx, sc.shape, base, fx);
     R w[3][3];
     bspline(fx, w);
-    Stencil<T> st;
-    st.init(ctx, sc, ax, tp.tile_slot, base);
+    DenseStencil st;
+    st.init(sc, ax, base);
+    const R* __restrict__ dense = static_cast<const R*>(ctx.dense_f);
     // nC = k4 sum w g (o - fx)^T dx = k4 dx (G - nv fx^T),  G[i][d] = sum w g_i o_d
     R nv[3] = {0, 0, 0}, G[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
 #pragma unroll
-    for (int a = 0; a < 3; ++a)
+    for (int a = 0; a < 3; ++a) {
+        if (!st.vx[a]) continue;
 #pragma unroll
         for (int b = 0; b < 3; ++b) {
-            long long r0, r1;
-            st.column(a, b, r0, r1);
+            if (!st.vy[b]) continue;
+            const long long rab = st.ox[a] + st.oy[b];
+            const R wab = w[a][0] * w[b][1];
 #pragma unroll
             for (int c = 0; c < 3; ++c) {
-                long long r = st.node(r0, r1, c);
-                if (r < 0) continue;
+                if (!st.vz[c]) continue;
                 R g[4];
-                load_node(tp.grid, r, g);
-                const R wt = w[a][0] * w[b][1] * w[c][2];
+                load_node(dense, rab + st.oz[c], g);
+                const R wt = wab * w[c][2];
 #pragma unroll
                 for (int i = 0; i < 3; ++i) {
                     const R wg = wt * g[1 + i];
@@ -632,6 +599,7 @@ g2p_kernel(Ctx ctx, Tape<R> tp, MpmParticles in, MpmParticles out, int advect) {
                 }
             }
         }
+    }
     R nC[9];
     const R kd = k4 * dx;
 #pragma unroll
@@ -706,7 +674,7 @@ bwd_payload_kernel(Ctx ctx, const unsigned* __restrict__ perm, MpmParticles in, 
 // ---------------------------------------------------------------------------
 template <typename R, int T>
 __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 2 : 1)
-bwd_particle_kernel(Ctx ctx, Tape<R> tp, const R* __restrict__ gridb, MpmParticles in, const R* __restrict__ outC,
+bwd_particle_kernel(Ctx ctx, Tape<R> tp, MpmParticles in, const R* __restrict__ outC,
                     MpmCotangents ob, MpmCotangents ib, double* __restrict__ dA, int advect, int t) {
     long long sidx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (sidx >= ctx.n) return;
@@ -758,26 +726,28 @@ bwd_particle_kernel(Ctx ctx, Tape<R> tp, const R* __restrict__ gridb, MpmParticl
     R w[3][3], dw[3][3];
     bspline(fx, w);
     bspline_grad(fx, dw);
-    Stencil<T> st;
-    st.init(ctx, sc, ax, tp.tile_slot, base);
+    DenseStencil st;
+    st.init(sc, ax, base);
+    const R* __restrict__ dfw = static_cast<const R*>(ctx.dense_f);
+    const R* __restrict__ dbw = static_cast<const R*>(ctx.dense_b);
 
     // Sb = sum w mb (o - fx)^T dx = dx (GB - wmb fx^T),  GB[i][d] = sum w mb_i o_d
     R xb[3] = {0, 0, 0}, wgv[3] = {0, 0, 0}, wmb[3] = {0, 0, 0}, GB[9];
 #pragma unroll
     for (int i = 0; i < 9; ++i) GB[i] = R(0);
 #pragma unroll
-    for (int a = 0; a < 3; ++a)
+    for (int a = 0; a < 3; ++a) {
+        if (!st.vx[a]) continue;
 #pragma unroll
         for (int b = 0; b < 3; ++b) {
-            long long r0, r1;
-            st.column(a, b, r0, r1);
+            if (!st.vy[b]) continue;
+            const long long rab = st.ox[a] + st.oy[b];
 #pragma unroll
             for (int cc = 0; cc < 3; ++cc) {
-                long long r = st.node(r0, r1, cc);
-                if (r < 0) continue;
+                if (!st.vz[cc]) continue;
                 R gf[4], gb[4];
-                load_node(tp.grid, r, gf);
-                load_node(gridb, r, gb);
+                load_node(dfw, rab + st.oz[cc], gf);
+                load_node(dbw, rab + st.oz[cc], gb);
                 const R wt = w[a][0] * w[b][1] * w[cc][2];
                 const R* gv = gf + 1;
                 const R* mb = gb + 1;
@@ -806,6 +776,7 @@ bwd_particle_kernel(Ctx ctx, Tape<R> tp, const R* __restrict__ gridb, MpmParticl
                 }
             }
         }
+    }
     R Sb[9];
 #pragma unroll
     for (int i = 0; i < 3; ++i)

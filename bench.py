@@ -336,7 +336,7 @@ def main():
     line["fp64_hencky_fallbacks_per_trajectory"] = fallbacks / max(1, a.warmup + a.steps + 3)
 
     if rank == 0 and not a.no_plain:
-        line["fp64_plain"] = plain_leg(scn, a, value)
+        line["fp64_plain"] = plain_leg(scn, a, value, tuning)
     if rank == 0 and not a.no_cpu:
         line["cpu_baseline"] = cpu_baseline(scn, a.cpu_seconds)
     if rank == 0:
@@ -347,7 +347,7 @@ def main():
         dist.destroy_process_group()
 
 
-def plain_leg(scn, a, value32):
+def plain_leg(scn, a, value32, tuning32=None):
     """FP64 plain path: one scene at a time, eager launches per step (the
     drop-in transfer path), same trajectory.  Timed on a sample of scenes
     spread over the size range; FP32 error vs FP64 on the same scenes."""
@@ -368,7 +368,7 @@ def plain_leg(scn, a, value32):
         torch.cuda.synchronize()
         secs += time.perf_counter() - t0
         units += s["x"].shape[0] * a.mpm_steps
-        b32 = Batch([s], a.mpm_steps, dtype=torch.float32, ckpt_every="auto")
+        b32 = Batch([s], a.mpm_steps, dtype=torch.float32, ckpt_every="auto", tuning=tuning32)
         b32.load(host_slab([s], np.float32), non_blocking=False)
         b32.run()
         torch.cuda.synchronize()

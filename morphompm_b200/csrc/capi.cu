@@ -186,7 +186,7 @@ int launch_p2g(MpmPlan* P, int mode, const Ctx& ctx, const R* payload, const int
     void* a2[] = {(void*)&ctx, (void*)&Sc, (void*)&cap, (void*)&active, (void*)&nact, (void*)&grid_out,
                   (void*)&grid_fwd, (void*)&advect};
     P->launches += 1;   // the Site around this call counts one
-    return cudaLaunchKernel(f2, dim3(ctas), dim3(256), a2, 0, st) == cudaSuccess ? MPM_OK : MPM_ERR_CUDA;
+    return cudaLaunchKernel(f2, dim3(ctas), dim3(1024), a2, 0, st) == cudaSuccess ? MPM_OK : MPM_ERR_CUDA;
 }
 
 // stable LSD radix sort of the binning keys -> tape (skeys, perm)
@@ -321,12 +321,12 @@ int mpm_plan_create(const MpmScene* scenes, int32_t n_scenes, int32_t real_bytes
     P->real_bytes = real_bytes;
     if (tuning) P->tune = *tuning;
     if (P->tune.tile_xy != 4 && P->tune.tile_xy != 16) P->tune.tile_xy = 8;
-    if (P->tune.scatter_ctas_per_sm <= 0) P->tune.scatter_ctas_per_sm = 4;
+    if (P->tune.scatter_ctas_per_sm <= 0) P->tune.scatter_ctas_per_sm = 1;
     if (P->tune.scatter_oxb != 1 && P->tune.scatter_oxb != 3) P->tune.scatter_oxb = real_bytes == 4 ? 3 : 1;
     if (real_bytes == 8) P->tune.scatter_oxb = 1;
     if (P->tune.particle_block <= 0 || P->tune.particle_block > 1024 || P->tune.particle_block % 32)
         P->tune.particle_block = 256;
-    if (P->tune.fp64_gap_thresh == 0.0f) P->tune.fp64_gap_thresh = 1e-4f;
+    if (P->tune.fp64_gap_thresh == 0.0f) P->tune.fp64_gap_thresh = 1e-6f;
     const int T = P->tune.tile_xy;
     P->TN = T * T * TILE_Z;
     long long cell = 0, tile = 0, pcur = 0, nodes = 0;
@@ -555,7 +555,7 @@ int mpm_stress(const MpmScene* scene, int32_t real_bytes, int64_t n, const void*
     int g = grid_for(n, 256);
     if (real_bytes == 4)
         stress_kernel<float><<<g, 256, 0, st>>>(*scene, n, (const float*)F, (const float*)Fg, (const float*)C,
-                                                (float*)tau, 1e-4f);
+                                                (float*)tau, 1e-6f);
     else
         stress_kernel<double><<<g, 256, 0, st>>>(*scene, n, (const double*)F, (const double*)Fg,
                                                  (const double*)C, (double*)tau, 0.0f);
@@ -572,7 +572,7 @@ int mpm_stress_vjp(const MpmScene* scene, int32_t real_bytes, int64_t n, const v
     if (real_bytes == 4)
         stress_vjp_kernel<float><<<g, 256, 0, st>>>(*scene, n, (const float*)F, (const float*)Fg, (const float*)C,
                                                     (const float*)tau_bar, (float*)F_bar, (float*)Fg_bar,
-                                                    (float*)C_bar, 1e-4f);
+                                                    (float*)C_bar, 1e-6f);
     else
         stress_vjp_kernel<double><<<g, 256, 0, st>>>(*scene, n, (const double*)F, (const double*)Fg,
                                                      (const double*)C, (const double*)tau_bar, (double*)F_bar,
@@ -669,10 +669,10 @@ int noalloc_scratch(void** out, int* n_sm) {
 bool noalloc_layout(MpmPlan& P, const MpmScene& sc, int real_bytes, SceneAux& a) {
     P.real_bytes = real_bytes;
     P.tune.tile_xy = 8;
-    P.tune.scatter_ctas_per_sm = 2;
+    P.tune.scatter_ctas_per_sm = 1;
     P.tune.scatter_oxb = real_bytes == 4 ? 3 : 1;
     P.tune.particle_block = 256;
-    P.tune.fp64_gap_thresh = 1e-4f;
+    P.tune.fp64_gap_thresh = 1e-6f;
     const int T = P.tune.tile_xy;
     P.TN = T * T * TILE_Z;
     a.cell_begin = 0;

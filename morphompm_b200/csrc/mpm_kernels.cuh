@@ -300,7 +300,7 @@ seg_write_kernel(Ctx ctx, const unsigned* __restrict__ skeys) {
 // record: fx[0..2], pmass, a = pmass v, B = (pmass C + dt sk) dx
 // ---------------------------------------------------------------------------
 template <typename R>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 3)
 prepass_kernel(Ctx ctx, MpmParticles P, const unsigned* __restrict__ perm, R* __restrict__ payload, int t) {
     long long sidx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (sidx >= ctx.n) return;
@@ -442,7 +442,7 @@ __device__ __forceinline__ void load_sum(const R* __restrict__ S, long long idx,
 }
 
 template <typename R, int T, int MODE>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(1024)
 node_sums_kernel(Ctx ctx, const R* __restrict__ S, long long cap, const int* __restrict__ active,
                  const int* __restrict__ n_active, R* __restrict__ grid_out, const R* __restrict__ grid_fwd,
                  int advect) {

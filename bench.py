@@ -44,6 +44,9 @@ def parse():
     ap.add_argument("--no-plain", action="store_true", help="skip the FP64 plain-path leg")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--workload", default="config4", choices=["config1", "config2", "config3", "config4", "config5"],
+                    help="config4 is the headline line; the others print one line each for the other growth "
+                         "workloads (FP64 and FP32 where the workload names both)")
     return ap.parse_args()
 
 
@@ -155,8 +158,20 @@ def run_reference(a):
     import multiprocessing as mp
     ctx = mp.get_context("spawn")
     steps = 2
-    picked, _ = cpu_sample(scn, 4.0, steps)        # per-core budget ~4 s of work per bench step
-    jobs = [(scn[i], steps) for i in picked[:max(cores * 2, 1)]]
+    # ~8 s of single-core work per process per bench step, scenes taken evenly
+    # over the size range of the workload
+    _, t1 = _oracle_scene_run((scn[0], steps))
+    rate = scn[0]["x"].shape[0] * steps / max(t1, 1e-6)
+    budget = rate * 8.0 * cores
+    order = sorted(range(len(scn)), key=lambda i: scn[i]["x"].shape[0])
+    stride = max(1, len(order) // 64)
+    jobs, acc = [], 0
+    for i in order[::stride]:
+        u = scn[i]["x"].shape[0] * steps
+        if acc + u > budget and jobs:
+            break
+        jobs.append((scn[i], steps))
+        acc += u
     vals = []
     with ctx.Pool(cores) as pool:
         for it in range(a.warmup + a.steps):
@@ -204,6 +219,8 @@ def main():
     a = parse()
     if a.impl == "reference":
         return run_reference(a)
+    if a.workload != "config4":
+        return run_other(a)
     import torch
     import torch.distributed as dist
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -263,10 +280,8 @@ def main():
     ms = e0.elapsed_time(e1)
     clk = clocks.stop()
     prof = plan.profile_end()
-    if world > 1:
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    from morphompm_b200.shard import max_over_ranks
+    ms = max_over_ranks(ms, dev)
     ms_per = ms / a.steps
     units = n_tot * a.mpm_steps * world
     value = units / (ms_per / 1e3)
@@ -287,10 +302,7 @@ def main():
     e1.record(s)
     torch.cuda.synchronize()
     ms_e2e = e0.elapsed_time(e1)
-    if world > 1:
-        t = torch.tensor([ms_e2e], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_e2e = float(t.item())
+    ms_e2e = max_over_ranks(ms_e2e, dev)
     e2e = {"value": units / (ms_e2e / a.steps / 1e3), "unit": UNIT,
            "h2d_bytes_per_step": int(slab_h.numel() * slab_h.element_size()),
            "d2h_bytes_per_step": int(2 * 8 * len(scn))}
@@ -345,6 +357,101 @@ def main():
         b.graph = None
         dist.barrier()
         dist.destroy_process_group()
+
+
+def _timed_trajectories(b, steps, warmup):
+    """Capture the batch's trajectory once, replay warmup + steps times; device
+    ms per trajectory (CUDA events on the replay stream)."""
+    import torch
+    b.capture()
+    for _ in range(warmup):
+        b.replay()
+    s = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(s)
+    for _ in range(steps):
+        b.replay()
+    e1.record(s)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / steps
+
+
+def _curvature(final_slab):
+    """Bending of the bilayer strip: least-squares parabola y(x) of the
+    centreline (mean y per x-bin), curvature ~ 2a (the measure of the
+    reference's Timoshenko test, tests/test_growth.cpp)."""
+    x = final_slab[0].astype(np.float64)
+    y = final_slab[1].astype(np.float64)
+    nb = 9
+    lo, hi = x.min(), x.max()
+    idx = np.minimum(nb - 1, ((x - lo) / ((hi - lo) / nb + 1e-12)).astype(int))
+    xm = np.array([x[idx == b].mean() for b in range(nb) if np.any(idx == b)])
+    ym = np.array([y[idx == b].mean() for b in range(nb) if np.any(idx == b)])
+    a2 = np.polyfit(xm - xm.mean(), ym, 2)[0]
+    return abs(2 * a2)
+
+
+def run_other(a):
+    """One JSON line for configs 1, 2, 3 or 5 (particle-steps/s fwd+adj)."""
+    import torch
+    from morphompm_b200 import scenes as S
+    from morphompm_b200.batch import Batch, host_slab
+    from morphompm_b200.trajectory import sqrt_schedule
+    w = a.workload
+    c = getattr(S, w)()
+    n = c["x"].shape[0]
+    line = {"metric": METRIC, "unit": UNIT, "workload": w, "name": c["name"], "n_gpus": 1, "steps": a.steps,
+            "warmup": a.warmup, "higher_is_better": True, "data": "synthetic", "particles": n,
+            "mpm_steps": c["steps"], "results": {}}
+    loss, x_obs = "detF", None
+    if w == "config3":
+        # observation: final positions of the g* trajectory; gradient at g_eval
+        c_true = dict(c, growth_A=c["g_true"] - 1.0, ramp_steps=0)
+        ob = Batch([c_true], c["steps"], dtype=torch.float64, ckpt_every=c["ckpt_every"])
+        ob.load(host_slab([c_true], np.float64), non_blocking=False)
+        ob.rollout.forward(ob.slab0)
+        x_obs = ob.rollout.final[0:3].t().cpu().numpy()
+        c = dict(c, growth_A=c["g_eval"] - 1.0, ramp_steps=0)
+        loss = "mse"
+        del ob
+    dtypes = {"config1": [torch.float64, torch.float32], "config2": [torch.float64, torch.float32],
+              "config3": [torch.float64, torch.float32], "config5": [torch.float32]}[w]
+    finals = {}
+    for dt in dtypes:
+        ck = {"config1": "auto", "config2": "auto", "config3": c.get("ckpt_every", 20),
+              "config5": sqrt_schedule(c["steps"])}[w]
+        if w == "config5":
+            # 80 GB memory cap for the whole trajectory storage
+            b = Batch([c], c["steps"], dtype=dt, ckpt_every=ck, loss=loss, x_obs=x_obs)
+        else:
+            b = Batch([c], c["steps"], dtype=dt, ckpt_every=ck, loss=loss, x_obs=x_obs)
+        npd = np.float64 if dt == torch.float64 else np.float32
+        b.load(host_slab([c], npd), non_blocking=False)
+        ms = _timed_trajectories(b, a.steps, a.warmup)
+        key = "fp64" if dt == torch.float64 else "fp32"
+        mem = b.rollout.memory_bytes() + b.plan.ws_bytes
+        res = {"value": n * c["steps"] / (ms / 1e3), "ms_per_trajectory": ms, "ckpt_every": b.ckpt_every,
+               "trajectory_storage_gb": round(mem / 1e9, 2), "loss": float(b.loss[0]),
+               "dloss_dg": float(b.dloss_dg[0]), "device_status": b.plan.status(),
+               "fp64_hencky_fallbacks": b.plan.fp64_fallbacks()}
+        finals[key] = b.rollout.final.double().cpu().numpy()
+        if w == "config2":
+            res["curvature"] = _curvature(finals[key])
+            res["curvature_timoshenko"] = 1.5 * 0.2 / (8 * c["dx"])
+        line["results"][key] = res
+        del b
+        torch.cuda.empty_cache()
+    if "fp64" in finals and "fp32" in finals:
+        f64, f32 = finals["fp64"], finals["fp32"]
+        g64, g32 = line["results"]["fp64"]["dloss_dg"], line["results"]["fp32"]["dloss_dg"]
+        line["fp32_error_vs_fp64"] = {"F": float(np.max(np.abs(f64[15:24] - f32[15:24]))),
+                                      "x": float(np.max(np.abs(f64[0:3] - f32[0:3]))),
+                                      "dLdg_rel": abs(g64 - g32) / max(abs(g64), 1e-300)}
+    main_key = "fp32" if "fp32" in line["results"] else "fp64"
+    line["value"] = line["results"][main_key]["value"]
+    line["dtype"] = "f32" if main_key == "fp32" else "f64"
+    print(json.dumps(line), flush=True)
 
 
 def plain_leg(scn, a, value32, tuning32=None):

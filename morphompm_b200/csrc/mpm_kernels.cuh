@@ -164,9 +164,9 @@ constexpr int SEG_ITEMS = 16;
 constexpr int SEG_TILE = SEG_THREADS * SEG_ITEMS;
 
 __device__ __forceinline__ void decode_cell(const MpmScene& sc, long long c, int cell[3]) {
-    long long P1 = sc.shape[1] + 2, P2 = sc.shape[2] + 2;
-    cell[2] = (int)(c % P2);
-    long long r = c / P2;
+    const unsigned P1 = sc.shape[1] + 2, P2 = sc.shape[2] + 2, u = (unsigned)c;
+    const unsigned r = u / P2;
+    cell[2] = (int)(u - r * P2);
     cell[1] = (int)(r % P1);
     cell[0] = (int)(r / P1);
 }
@@ -201,14 +201,16 @@ __device__ __forceinline__ void flag_tiles(const Ctx& ctx, long long s, unsigned
                 ctx.tile_flag[ax.tile_begin + ((long long)a * ax.ntile[1] + b) * ax.ntile[2] + e] = 1;
 }
 
+// Slots of a block are visited warp-striped (slot = block base + round*256 +
+// thread), so every load of the sorted keys is coalesced.
 __global__ void __launch_bounds__(SEG_THREADS)
 seg_count_kernel(Ctx ctx, const unsigned* __restrict__ skeys, int flag) {
-    __shared__ unsigned red[SEG_THREADS];
-    const long long base = (long long)blockIdx.x * SEG_TILE + (long long)threadIdx.x * SEG_ITEMS;
+    __shared__ unsigned red[SEG_THREADS / 32];
+    const long long base = (long long)blockIdx.x * SEG_TILE;
     unsigned cnt = 0;
 #pragma unroll 4
-    for (int i = 0; i < SEG_ITEMS; ++i) {
-        long long s = base + i;
+    for (int r = 0; r < SEG_ITEMS; ++r) {
+        long long s = base + (long long)r * SEG_THREADS + threadIdx.x;
         if (s >= ctx.n) break;
         unsigned k = skeys[s];
         if (seg_start(ctx, skeys, s, k)) {
@@ -216,13 +218,14 @@ seg_count_kernel(Ctx ctx, const unsigned* __restrict__ skeys, int flag) {
             if (flag) flag_tiles(ctx, s, k);
         }
     }
-    red[threadIdx.x] = cnt;
+    for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = cnt;
     __syncthreads();
-    for (int w = SEG_THREADS / 2; w > 0; w >>= 1) {
-        if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
-        __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned t = 0;
+        for (int w = 0; w < SEG_THREADS / 32; ++w) t += red[w];
+        ctx.blk_count[blockIdx.x] = t;
     }
-    if (threadIdx.x == 0) ctx.blk_count[blockIdx.x] = red[0];
 }
 
 // exclusive scan of the block counts in place; total -> *n_seg (single block)
@@ -254,44 +257,44 @@ seg_scan_kernel(Ctx ctx, int nblk) {
 
 __global__ void __launch_bounds__(SEG_THREADS)
 seg_write_kernel(Ctx ctx, const unsigned* __restrict__ skeys) {
-    __shared__ unsigned sh[SEG_THREADS];
-    const long long base = (long long)blockIdx.x * SEG_TILE + (long long)threadIdx.x * SEG_ITEMS;
-    unsigned cnt = 0;
-    unsigned flags = 0;
+    constexpr int NW = SEG_THREADS / 32;
+    __shared__ unsigned wtot[NW];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const unsigned lt = (1u << lane) - 1u;
+    const long long base = (long long)blockIdx.x * SEG_TILE;
+    unsigned run = ctx.blk_count[blockIdx.x];     // segments started before this round
+    for (int r = 0; r < SEG_ITEMS; ++r) {
+        const long long s = base + (long long)r * SEG_THREADS + threadIdx.x;
+        const bool valid = s < ctx.n;
+        const unsigned k = valid ? skeys[s] : 0u;
+        const bool start = valid && seg_start(ctx, skeys, s, k);
+        const unsigned ball = __ballot_sync(0xffffffffu, start);
+        if (lane == 0) wtot[warp] = __popc(ball);
+        __syncthreads();
+        unsigned before = run;
+        unsigned round = 0;
 #pragma unroll
-    for (int i = 0; i < SEG_ITEMS; ++i) {
-        long long s = base + i;
-        if (s < ctx.n && seg_start(ctx, skeys, s, skeys[s])) {
-            ++cnt;
-            flags |= 1u << i;
+        for (int w = 0; w < NW; ++w) {
+            const unsigned c = wtot[w];
+            if (w < warp) before += c;
+            round += c;
         }
-    }
-    sh[threadIdx.x] = cnt;
-    __syncthreads();
-    for (int o = 1; o < SEG_THREADS; o <<= 1) {
-        unsigned t = threadIdx.x >= (unsigned)o ? sh[threadIdx.x - o] : 0u;
+        before += __popc(ball & lt);
+        // starts up to and including s, minus one: the segment id of slot s
+        const unsigned id = before + (start ? 1u : 0u);
+        if (start) {
+            ctx.seg_first[id - 1] = (int)s;
+            ctx.cell_seg[k] = (int)id;
+        }
+        if (valid && id > 0) {
+            const bool last = s == ctx.n - 1 || skeys[s + 1] != k;
+            if (last) {
+                const SceneAux& ax = ctx.aux[ctx.scene_of[s]];
+                if ((long long)k - ax.cell_begin < ax.ncells) ctx.seg_last[id - 1] = (int)(s + 1);
+            }
+        }
+        run += round;
         __syncthreads();
-        sh[threadIdx.x] += t;
-        __syncthreads();
-    }
-    // segments started before this thread's first slot
-    unsigned run = ctx.blk_count[blockIdx.x] + sh[threadIdx.x] - cnt;
-#pragma unroll 4
-    for (int i = 0; i < SEG_ITEMS; ++i) {
-        long long s = base + i;
-        if (s >= ctx.n) break;
-        unsigned k = skeys[s];
-        if (flags & (1u << i)) {
-            ctx.seg_first[run] = (int)s;
-            ctx.cell_seg[k] = (int)run + 1;
-            ++run;
-        }
-        bool last = s == ctx.n - 1 || skeys[s + 1] != k;
-        if (last && run > 0) {
-            // the slot belongs to segment run-1 only if its key is inside
-            const SceneAux& ax = ctx.aux[ctx.scene_of[s]];
-            if ((long long)k - ax.cell_begin < ax.ncells) ctx.seg_last[run - 1] = (int)(s + 1);
-        }
     }
 }
 

@@ -9,7 +9,7 @@
 
 namespace mpm {
 
-constexpr int RADIX_BITS = 8;
+constexpr int RADIX_BITS = 9;
 constexpr int RADIX = 1 << RADIX_BITS;
 constexpr int SORT_THREADS = 256;
 constexpr int SORT_ITEMS = 16;                       // keys per thread per block
@@ -53,8 +53,10 @@ radix_rowscan_kernel(unsigned* __restrict__ hist, int nblk, const unsigned* __re
     __shared__ unsigned sh[256];
     __shared__ unsigned carry;
     int d = blockIdx.x;
-    // digit offset
-    sh[threadIdx.x] = (threadIdx.x < (unsigned)d) ? totals[threadIdx.x] : 0u;
+    // digit offset: sum of the totals of the smaller digits
+    unsigned part = 0;
+    for (int e = threadIdx.x; e < d; e += 256) part += totals[e];
+    sh[threadIdx.x] = part;
     __syncthreads();
     for (int w = 128; w > 0; w >>= 1) {
         if (threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];

@@ -168,6 +168,20 @@ void* nodes_fn(int T) {
     return (void*)node_sums_kernel<R, 8, MODE>;
 }
 
+// P2G phase 2 (node gather + grid epilogue) over the active tiles
+template <typename R>
+int launch_nodes(MpmPlan* P, int mode, const Ctx& ctx, const int* active, const int* nact, R* grid_out,
+                 const R* grid_fwd, int advect, cudaStream_t st) {
+    const R* Sc = at<R>(P, P->o_sums);
+    long long cap = P->n;
+    int ctas = P->n_sm * std::max(1, P->tune.scatter_ctas_per_sm);
+    ctas = std::max(1, std::min(ctas, P->active_cap));
+    void* f2 = mode == 0 ? nodes_fn<R, 0>(P->tune.tile_xy) : nodes_fn<R, 1>(P->tune.tile_xy);
+    void* a2[] = {(void*)&ctx, (void*)&Sc, (void*)&cap, (void*)&active, (void*)&nact, (void*)&grid_out,
+                  (void*)&grid_fwd, (void*)&advect};
+    return cudaLaunchKernel(f2, dim3(ctas), dim3(1024), a2, 0, st) == cudaSuccess ? MPM_OK : MPM_ERR_CUDA;
+}
+
 // two-phase P2G: per-cell stencil sums, then per-node gather + grid epilogue
 template <typename R>
 int launch_p2g(MpmPlan* P, int mode, const Ctx& ctx, const R* payload, const int* active, const int* nact,
@@ -179,14 +193,8 @@ int launch_p2g(MpmPlan* P, int mode, const Ctx& ctx, const R* payload, const int
     void* f1 = mode == 0 ? sums_fn<R, 0>(P->tune.scatter_oxb) : sums_fn<R, 1>(P->tune.scatter_oxb);
     void* a1[] = {(void*)&ctx, (void*)&payload, (void*)&S, (void*)&cap};
     if (cudaLaunchKernel(f1, dim3(blocks1), dim3(128), a1, 0, st) != cudaSuccess) return MPM_ERR_CUDA;
-    const R* Sc = S;
-    int ctas = P->n_sm * std::max(1, P->tune.scatter_ctas_per_sm);
-    ctas = std::max(1, std::min(ctas, P->active_cap));
-    void* f2 = mode == 0 ? nodes_fn<R, 0>(P->tune.tile_xy) : nodes_fn<R, 1>(P->tune.tile_xy);
-    void* a2[] = {(void*)&ctx, (void*)&Sc, (void*)&cap, (void*)&active, (void*)&nact, (void*)&grid_out,
-                  (void*)&grid_fwd, (void*)&advect};
     P->launches += 1;   // the Site around this call counts one
-    return cudaLaunchKernel(f2, dim3(ctas), dim3(1024), a2, 0, st) == cudaSuccess ? MPM_OK : MPM_ERR_CUDA;
+    return launch_nodes<R>(P, mode, ctx, active, nact, grid_out, grid_fwd, advect, st);
 }
 
 // stable LSD radix sort of the binning keys -> tape (skeys, perm)
@@ -251,19 +259,22 @@ int step_bwd_T(MpmPlan* P, const MpmParticles& in, const void* outC, const MpmCo
     Tape<R> tp = make_tape<R>(P, const_cast<char*>(tape));
     const int B = P->tune.particle_block;
     const int g = grid_for(P->n, B);
-    R* payload = at<R>(P, P->o_payload);
     double* dbuf = at<double>(P, P->o_dbuf);
     int rc = build_segments(P, ctx, tp.skeys, 0, st);
     if (rc) return rc;
     {
-        Site s(P, MPM_K_BWD_PAYLOAD, 1, st);
-        bwd_payload_kernel<R><<<g, B, 0, st>>>(ctx, tp.perm, in, ob, payload, advect);
-    }
-    rc = check_launch();
-    if (rc) return rc;
-    {
-        Site s(P, MPM_K_BWD_P2G, 1, st);
-        rc = launch_p2g<R>(P, 1, ctx, payload, tp.active, tp.n_active, nullptr, tp.grid, advect, st);
+        Site s(P, MPM_K_BWD_P2G, 2, st);
+        R* S = at<R>(P, P->o_sums);
+        long long cap = P->n;
+        int blocks1 = (int)std::min<long long>((P->n + 127) / 128, (long long)P->n_sm * 16);
+        blocks1 = std::max(1, blocks1);
+        if (P->tune.scatter_oxb == 3 && sizeof(R) == 4)
+            cell_sums_adj_kernel<R, 3><<<blocks1, 128, 0, st>>>(ctx, tp.perm, in, ob, S, cap, advect);
+        else
+            cell_sums_adj_kernel<R, 1><<<blocks1, 128, 0, st>>>(ctx, tp.perm, in, ob, S, cap, advect);
+        rc = check_launch();
+        if (rc) return rc;
+        rc = launch_nodes<R>(P, 1, ctx, tp.active, tp.n_active, nullptr, tp.grid, advect, st);
     }
     if (rc) return rc;
     bool want_dA = growth_grad != nullptr && P->any_growth;

@@ -11,8 +11,8 @@
 //                     in a fixed order, + grid update with boundary conditions
 //   g2p_kernel        gather, advect, F update; clears the cell marks
 // Reverse (python/morphompm/transfer.py:82-158):
-//   bwd_payload_kernel   G2P adjoint payload (nv_b, Cn_b') per particle
-//   cell/node_sums<1>    gv_b scatter + grid adjoint (gmom_b, gm_b)
+//   cell_sums_adj     gv_b scatter phase 1 (nv_b, Cn_b' formed per particle)
+//   node_sums<1>      gv_b gather + grid adjoint (gmom_b, gm_b)
 //   bwd_particle_kernel  P2G adjoint, constitutive VJP, volume path, x_b terms
 //
 // P2G determinism: particles are sorted by cell, every occupied cell's sums
@@ -426,6 +426,96 @@ cell_sums_kernel(Ctx ctx, const R* __restrict__ payload, R* __restrict__ S, long
 }
 
 // ---------------------------------------------------------------------------
+// Reverse P2G, phase 1 (transfer.py:99-119 scatter of gv_b): per occupied cell
+// the 27 stencil sums of w (nv_b + k4 Cn_b' dp), with nv_b = vn_b + dt xn_b
+// (advect) and Cn_b' = Cn_b + dt Fn_b F^T formed here from the cotangents of
+// the step's output, so no payload record is written for the reverse.
+// ---------------------------------------------------------------------------
+template <typename R, int OXB>
+__global__ void __launch_bounds__(128)
+cell_sums_adj_kernel(Ctx ctx, const unsigned* __restrict__ perm, MpmParticles in, MpmCotangents ob,
+                     R* __restrict__ S, long long cap, int advect) {
+    const int nseg = *ctx.n_seg;
+    for (int id = blockIdx.x * blockDim.x + threadIdx.x; id < nseg; id += gridDim.x * blockDim.x) {
+        const int first = ctx.seg_first[id], last = ctx.seg_last[id];
+        const MpmScene& sc = ctx.scenes[ctx.scene_of[first]];
+        const R dx = (R)sc.dx, dt = (R)sc.dt, inv_dx = (R)(1.0 / sc.dx);
+        const R kdx = R(4) * inv_dx * inv_dx * dx;
+#pragma unroll 1
+        for (int ox0 = 0; ox0 < 3; ox0 += OXB) {
+            R acc[OXB][3][3][3];
+#pragma unroll
+            for (int a = 0; a < OXB; ++a)
+#pragma unroll
+                for (int b = 0; b < 3; ++b)
+#pragma unroll
+                    for (int c = 0; c < 3; ++c)
+#pragma unroll
+                        for (int h = 0; h < 3; ++h) acc[a][b][c][h] = R(0);
+            for (int q = first; q < last; ++q) {
+                const long long p = perm[q];
+                R x[3], nv[3], B[9];
+                ld3<R>(in.x, p, in.sp3, in.sc3, x);
+                {
+                    R F[9], Fb[9], Cb[9], xb[3];
+                    ld9<R>(in.F, p, in.sp9, in.sc9, F);
+                    ld9<R>(ob.F, p, ob.sp9, ob.sc9, Fb);
+                    ld9<R>(ob.C, p, ob.sp9, ob.sc9, Cb);
+                    ld3<R>(ob.v, p, ob.sp3, ob.sc3, nv);
+                    if (advect) {
+                        ld3<R>(ob.x, p, ob.sp3, ob.sc3, xb);
+#pragma unroll
+                        for (int i = 0; i < 3; ++i) nv[i] += dt * xb[i];
+                    }
+                    R FbFt[9];
+                    mmT(Fb, F, FbFt);
+#pragma unroll
+                    for (int i = 0; i < 9; ++i) B[i] = kdx * (Cb[i] + dt * FbFt[i]);
+                }
+                int base[3];
+                R fx[3];
+                bin_particle(x, inv_dx, sc.shape, base, fx);
+                R w[3][3];
+                bspline(fx, w);
+                const R dz[3] = {R(0) - fx[2], R(1) - fx[2], R(2) - fx[2]};
+                const R dy[3] = {R(0) - fx[1], R(1) - fx[1], R(2) - fx[1]};
+#pragma unroll
+                for (int a = 0; a < OXB; ++a) {
+                    const int ox = ox0 + a;
+                    const R dpx = R(ox) - fx[0];
+                    R wx;
+                    if constexpr (OXB == 3) wx = w[a][0];
+                    else wx = ox == 0 ? w[0][0] : (ox == 1 ? w[1][0] : w[2][0]);
+                    const R ax0 = nv[0] + B[0] * dpx, ax1 = nv[1] + B[3] * dpx, ax2 = nv[2] + B[6] * dpx;
+#pragma unroll
+                    for (int oy = 0; oy < 3; ++oy) {
+                        const R wxy = wx * w[oy][1];
+                        const R ay0 = ax0 + B[1] * dy[oy], ay1 = ax1 + B[4] * dy[oy], ay2 = ax2 + B[7] * dy[oy];
+#pragma unroll
+                        for (int oz = 0; oz < 3; ++oz) {
+                            const R wt = wxy * w[oz][2];
+                            acc[a][oy][oz][0] += wt * (ay0 + B[2] * dz[oz]);
+                            acc[a][oy][oz][1] += wt * (ay1 + B[5] * dz[oz]);
+                            acc[a][oy][oz][2] += wt * (ay2 + B[8] * dz[oz]);
+                        }
+                    }
+                }
+            }
+#pragma unroll
+            for (int a = 0; a < OXB; ++a)
+#pragma unroll
+                for (int oy = 0; oy < 3; ++oy)
+#pragma unroll
+                    for (int oz = 0; oz < 3; ++oz) {
+                        const int o = 9 * (ox0 + a) + 3 * oy + oz;
+                        const R v4[4] = {acc[a][oy][oz][0], acc[a][oy][oz][1], acc[a][oy][oz][2], R(0)};
+                        store_sum(S, (long long)o * cap + id, v4);
+                    }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
 // P2G, phase 2: node gather + grid update.  One CTA per active node tile
 // (persistent over the active list); every node adds the sums of its 27
 // source cells in the fixed order o = 0..26, then
@@ -630,42 +720,6 @@ g2p_kernel(Ctx ctx, Tape<R> tp, MpmParticles in, MpmParticles out, int advect) {
     if (!finite9(Fn) || !(xn[0] * R(0) == R(0) && xn[1] * R(0) == R(0) && xn[2] * R(0) == R(0)))
         raise_status(ctx.status, MPM_ERR_NONFINITE);
     unmark_cell(ctx, ax, tp.skeys, sidx);
-}
-
-// ---------------------------------------------------------------------------
-// reverse: G2P-adjoint payload (transfer.py:99-119)
-// record: fx, m = 0, a = nv_b, B = k4 dx Cn_b'   with
-//   nv_b = vn_b + dt xn_b (advect),  Cn_b' = Cn_b + dt Fn_b F^T
-// ---------------------------------------------------------------------------
-template <typename R>
-__global__ void __launch_bounds__(256)
-bwd_payload_kernel(Ctx ctx, const unsigned* __restrict__ perm, MpmParticles in, MpmCotangents ob,
-                   R* __restrict__ payload, int advect) {
-    long long sidx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (sidx >= ctx.n) return;
-    long long p = perm[sidx];
-    const MpmScene& sc = ctx.scenes[ctx.scene_of[sidx]];
-    const R dx = (R)sc.dx, dt = (R)sc.dt, inv_dx = (R)(1.0 / sc.dx);
-    const R k4 = R(4) * inv_dx * inv_dx;
-    R x[3], F[9], xb[3], vb[3], Cb[9], Fb[9];
-    ld3<R>(in.x, p, in.sp3, in.sc3, x);
-    ld9<R>(in.F, p, in.sp9, in.sc9, F);
-    ld3<R>(ob.x, p, ob.sp3, ob.sc3, xb);
-    ld3<R>(ob.v, p, ob.sp3, ob.sc3, vb);
-    ld9<R>(ob.C, p, ob.sp9, ob.sc9, Cb);
-    ld9<R>(ob.F, p, ob.sp9, ob.sc9, Fb);
-    int base[3];
-    R fx[3];
-    bin_particle(x, inv_dx, sc.shape, base, fx);
-    R FbFt[9];
-    mmT(Fb, F, FbFt);
-    R rec[PAYLOAD];
-    rec[0] = fx[0]; rec[1] = fx[1]; rec[2] = fx[2]; rec[3] = R(0);
-#pragma unroll
-    for (int i = 0; i < 3; ++i) rec[4 + i] = advect ? vb[i] + dt * xb[i] : vb[i];
-#pragma unroll
-    for (int i = 0; i < 9; ++i) rec[7 + i] = k4 * (Cb[i] + dt * FbFt[i]) * dx;
-    store_record(payload, sidx, rec);
 }
 
 // ---------------------------------------------------------------------------

@@ -335,8 +335,8 @@ int mpm_plan_create(const MpmScene* scenes, int32_t n_scenes, int32_t real_bytes
     if (P->tune.scatter_ctas_per_sm <= 0) P->tune.scatter_ctas_per_sm = 1;
     if (P->tune.scatter_oxb != 1 && P->tune.scatter_oxb != 3) P->tune.scatter_oxb = real_bytes == 4 ? 3 : 1;
     if (real_bytes == 8) P->tune.scatter_oxb = 1;
-    if (P->tune.particle_block <= 0 || P->tune.particle_block > 1024 || P->tune.particle_block % 32)
-        P->tune.particle_block = 256;
+    // the per-particle kernels are compiled for at most 256 threads per block
+    if (P->tune.particle_block != 64 && P->tune.particle_block != 128) P->tune.particle_block = 256;
     if (P->tune.fp64_gap_thresh == 0.0f) P->tune.fp64_gap_thresh = 1e-6f;
     const int T = P->tune.tile_xy;
     P->TN = T * T * TILE_Z;

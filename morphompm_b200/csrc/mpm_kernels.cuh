@@ -646,7 +646,7 @@ __device__ __forceinline__ void unmark_cell(const Ctx& ctx, const SceneAux& ax, 
 // the input's particle order and clears the cell marks of this step.
 // ---------------------------------------------------------------------------
 template <typename R, int T>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 4)
 g2p_kernel(Ctx ctx, Tape<R> tp, MpmParticles in, MpmParticles out, int advect) {
     long long sidx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (sidx >= ctx.n) return;

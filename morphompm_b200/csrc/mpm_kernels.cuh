@@ -785,13 +785,26 @@ bwd_particle_kernel(Ctx ctx, Tape<R> tp, MpmParticles in, const R* __restrict__ 
     bspline_grad(fx, dw);
     DenseStencil st;
     st.init(sc, ax, base);
+
+    // The node loop is evaluated as separable sums: per stencil column (a,b)
+    // the z-weighted sums of gv, mb and c*mb, and of the advect factor
+    //   sfac(o) = gv.U(o) + mb.V(o) + pm gm_b,  U(o) = nv_b + M1^T dp, V(o) = pm v + M2^T dp
+    // (dp = (o - fx) dx, so U and V are affine in o: U = U0 + dx (a M1_0 + b M1_1 + c M1_2)
+    // with M1_i the rows of M1), then the column sums are weighted by w_a w_b.
+    // Sb = sum w mb (o - fx)^T dx = dx (GB - wmb fx^T),  GB[i][d] = sum w mb_i o_d
+    R D1[9], D2[9], U0[3], V0[3];
+#pragma unroll
+    for (int q = 0; q < 9; ++q) { D1[q] = dx * M1[q]; D2[q] = dx * M2[q]; }
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+        U0[j] = nvb[j] - (D1[j] * fx[0] + D1[3 + j] * fx[1] + D1[6 + j] * fx[2]);
+        V0[j] = pv[j] - (D2[j] * fx[0] + D2[3 + j] * fx[1] + D2[6 + j] * fx[2]);
+    }
     const R* __restrict__ dfw = static_cast<const R*>(ctx.dense_f);
     const R* __restrict__ dbw = static_cast<const R*>(ctx.dense_b);
-
-    // Sb = sum w mb (o - fx)^T dx = dx (GB - wmb fx^T),  GB[i][d] = sum w mb_i o_d
-    R xb[3] = {0, 0, 0}, wgv[3] = {0, 0, 0}, wmb[3] = {0, 0, 0}, GB[9];
+    R xs[3] = {0, 0, 0}, wgv[3] = {0, 0, 0}, wmb[3] = {0, 0, 0}, GB[9];
 #pragma unroll
-    for (int i = 0; i < 9; ++i) GB[i] = R(0);
+    for (int q = 0; q < 9; ++q) GB[q] = R(0);
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
         if (!st.vx[a]) continue;
@@ -799,41 +812,54 @@ bwd_particle_kernel(Ctx ctx, Tape<R> tp, MpmParticles in, const R* __restrict__ 
         for (int b = 0; b < 3; ++b) {
             if (!st.vy[b]) continue;
             const long long rab = st.ox[a] + st.oy[b];
+            R Zg[3] = {0, 0, 0}, Zm[3] = {0, 0, 0}, Zc[3] = {0, 0, 0}, Sab = 0, Tab = 0;
+            R Uab[3], Vab[3];
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+                Uab[j] = U0[j] + R(a) * D1[j] + R(b) * D1[3 + j];
+                Vab[j] = V0[j] + R(a) * D2[j] + R(b) * D2[3 + j];
+            }
 #pragma unroll
             for (int cc = 0; cc < 3; ++cc) {
                 if (!st.vz[cc]) continue;
                 R gf[4], gb[4];
                 load_node(dfw, rab + st.oz[cc], gf);
                 load_node(dbw, rab + st.oz[cc], gb);
-                const R wt = w[a][0] * w[b][1] * w[cc][2];
                 const R* gv = gf + 1;
                 const R* mb = gb + 1;
+                const R wz = w[cc][2];
 #pragma unroll
                 for (int i = 0; i < 3; ++i) {
-                    wgv[i] += wt * gv[i];
-                    const R wm = wt * mb[i];
-                    wmb[i] += wm;
-                    if (a) GB[3 * i + 0] += R(a) * wm;
-                    if (b) GB[3 * i + 1] += R(b) * wm;
-                    if (cc) GB[3 * i + 2] += R(cc) * wm;
+                    Zg[i] += wz * gv[i];
+                    Zm[i] += wz * mb[i];
+                    if (cc) Zc[i] += (R(cc) * wz) * mb[i];
                 }
                 if (advect) {
-                    const R dp[3] = {(R(a) - fx[0]) * dx, (R(b) - fx[1]) * dx, (R(cc) - fx[2]) * dx};
-                    R beta[3];
+                    R sfac = gb[0] * pm;
 #pragma unroll
-                    for (int i = 0; i < 3; ++i)
-                        beta[i] = M1[3 * i] * gv[0] + M1[3 * i + 1] * gv[1] + M1[3 * i + 2] * gv[2]
-                                + M2[3 * i] * mb[0] + M2[3 * i + 1] * mb[1] + M2[3 * i + 2] * mb[2];
-                    const R sfac = nvb[0] * gv[0] + nvb[1] * gv[1] + nvb[2] * gv[2]
-                                 + mb[0] * pv[0] + mb[1] * pv[1] + mb[2] * pv[2] + gb[0] * pm
-                                 + beta[0] * dp[0] + beta[1] * dp[1] + beta[2] * dp[2];
-                    xb[0] += sfac * (dw[a][0] * w[b][1] * w[cc][2] * inv_dx);
-                    xb[1] += sfac * (w[a][0] * dw[b][1] * w[cc][2] * inv_dx);
-                    xb[2] += sfac * (w[a][0] * w[b][1] * dw[cc][2] * inv_dx);
+                    for (int j = 0; j < 3; ++j)
+                        sfac += gv[j] * (Uab[j] + R(cc) * D1[6 + j]) + mb[j] * (Vab[j] + R(cc) * D2[6 + j]);
+                    Sab += wz * sfac;
+                    Tab += dw[cc][2] * sfac;
                 }
+            }
+            const R wab = w[a][0] * w[b][1];
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                wgv[i] += wab * Zg[i];
+                wmb[i] += wab * Zm[i];
+                if (a) GB[3 * i + 0] += (R(a) * wab) * Zm[i];
+                if (b) GB[3 * i + 1] += (R(b) * wab) * Zm[i];
+                GB[3 * i + 2] += wab * Zc[i];
+            }
+            if (advect) {
+                xs[0] += (dw[a][0] * w[b][1]) * Sab;
+                xs[1] += (w[a][0] * dw[b][1]) * Sab;
+                xs[2] += wab * Tab;
             }
         }
     }
+    R xb[3] = {xs[0] * inv_dx, xs[1] * inv_dx, xs[2] * inv_dx};
     R Sb[9];
 #pragma unroll
     for (int i = 0; i < 3; ++i)
@@ -858,8 +884,8 @@ bwd_particle_kernel(Ctx ctx, Tape<R> tp, MpmParticles in, const R* __restrict__ 
         ld3<R>(ob.x, p, ob.sp3, ob.sc3, xnb);
 #pragma unroll
         for (int i = 0; i < 3; ++i)
-            xb[i] += xnb[i] - (M1[3 * i] * wgv[0] + M1[3 * i + 1] * wgv[1] + M1[3 * i + 2] * wgv[2])
-                   - (M2[3 * i] * wmb[0] + M2[3 * i + 1] * wmb[1] + M2[3 * i + 2] * wmb[2]);
+            xb[i] += xnb[i] - inv_dx * (D1[3 * i] * wgv[0] + D1[3 * i + 1] * wgv[1] + D1[3 * i + 2] * wgv[2]
+                                      + D2[3 * i] * wmb[0] + D2[3 * i + 1] * wmb[1] + D2[3 * i + 2] * wmb[2]);
     }
 #pragma unroll
     for (int i = 0; i < 3; ++i) vb[i] = pm * wmb[i];

@@ -31,12 +31,30 @@ __device__ __forceinline__ bool jacobi_rotate(R A[3][3], R V[9], int p, int q) {
         A[q][p] = R(0);
         return false;
     }
-    R theta = (A[q][q] - A[p][p]) / (R(2) * apq);
-    R t = R(1) / (d_abs(theta) + d_sqrt(theta * theta + R(1)));
-    if (theta < R(0)) t = -t;
-    R c = R(1) / d_sqrt(t * t + R(1));
-    R s = t * c;
-    R tau = s / (R(1) + c);
+    R t, c, s, tau;
+    if constexpr (sizeof(R) == 4) {
+        // FP32: hardware reciprocal / reciprocal square root.  t need not be
+        // the exact tangent (the annihilated entry is set to zero, an error at
+        // rounding level); c gets one Newton step for 1/sqrt so that (c, s)
+        // stays a rotation to rounding level.
+        const float theta = __fdividef(A[q][q] - A[p][p], 2.0f * apq);
+        const float h2 = fmaf(theta, theta, 1.0f);
+        t = __fdividef(1.0f, fabsf(theta) + h2 * rsqrtf(h2));
+        if (theta < 0.0f) t = -t;
+        const float u = fmaf(t, t, 1.0f);
+        float r = rsqrtf(u);
+        r = r * fmaf(-0.5f * u * r, r, 1.5f);
+        c = r;
+        s = t * c;
+        tau = __fdividef(s, 1.0f + c);
+    } else {
+        R theta = (A[q][q] - A[p][p]) / (R(2) * apq);
+        t = R(1) / (d_abs(theta) + d_sqrt(theta * theta + R(1)));
+        if (theta < R(0)) t = -t;
+        c = R(1) / d_sqrt(t * t + R(1));
+        s = t * c;
+        tau = s / (R(1) + c);
+    }
     A[p][p] -= t * apq;
     A[q][q] += t * apq;
     A[p][q] = R(0);
@@ -165,9 +183,11 @@ __device__ __forceinline__ void hencky_tau_from_eig(const R beta[3], const R V[9
 #pragma unroll
     for (int i = 0; i < 3; ++i)
 #pragma unroll
-        for (int j = 0; j < 3; ++j)
+        for (int j = i; j < 3; ++j) {
             tau[3 * i + j] = V[3 * i] * h[0] * V[3 * j] + V[3 * i + 1] * h[1] * V[3 * j + 1]
                            + V[3 * i + 2] * h[2] * V[3 * j + 2];
+            tau[3 * j + i] = tau[3 * i + j];
+        }
 }
 
 template <typename R>
@@ -195,17 +215,36 @@ __device__ __forceinline__ void hencky_vjp_from_eig(const R F[9], const R Fgi[9]
     R M[9];
 #pragma unroll
     for (int i = 0; i < 9; ++i) M[i] = mu * tb[i] + ((i % 4 == 0) ? R(0.5) * lam * tr : R(0));
+    // M, V^T M V and V (. o L) V^T are symmetric: only the upper triangle is formed
     R T[9], UtMU[9];
     mTm(V, M, T);         // V^T M
-    mm(T, V, UtMU);       // V^T M V
-    R lb[3] = {d_log(beta[0]), d_log(beta[1]), d_log(beta[2])};
 #pragma unroll
     for (int i = 0; i < 3; ++i)
 #pragma unroll
-        for (int j = 0; j < 3; ++j) UtMU[3 * i + j] *= dk_entry<R>(beta[i], beta[j], lb[i], lb[j]);
+        for (int j = i; j < 3; ++j) {
+            UtMU[3 * i + j] = T[3 * i] * V[j] + T[3 * i + 1] * V[3 + j] + T[3 * i + 2] * V[6 + j];
+            UtMU[3 * j + i] = UtMU[3 * i + j];
+        }
+    R lb[3] = {d_log(beta[0]), d_log(beta[1]), d_log(beta[2])};
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        UtMU[4 * i] *= dk_entry<R>(beta[i], beta[i], lb[i], lb[i]);
+#pragma unroll
+        for (int j = i + 1; j < 3; ++j) {
+            const R L = dk_entry<R>(beta[i], beta[j], lb[i], lb[j]);
+            UtMU[3 * i + j] *= L;
+            UtMU[3 * j + i] *= L;
+        }
+    }
     R Bb[9];
     mm(V, UtMU, T);
-    mmT(T, V, Bb);        // V (UtMU o L) V^T
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = i; j < 3; ++j) {
+            Bb[3 * i + j] = T[3 * i] * V[3 * j] + T[3 * i + 1] * V[3 * j + 1] + T[3 * i + 2] * V[3 * j + 2];
+            Bb[3 * j + i] = Bb[3 * i + j];
+        }
     R Feb[9];
     mm(Bb, Fe, Feb);
 #pragma unroll

@@ -646,7 +646,7 @@ __device__ __forceinline__ void unmark_cell(const Ctx& ctx, const SceneAux& ax, 
 // the input's particle order and clears the cell marks of this step.
 // ---------------------------------------------------------------------------
 template <typename R, int T>
-__global__ void __launch_bounds__(256, 4)
+__global__ void __launch_bounds__(256, sizeof(R) == 4 ? 4 : 2)
 g2p_kernel(Ctx ctx, Tape<R> tp, MpmParticles in, MpmParticles out, int advect) {
     long long sidx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (sidx >= ctx.n) return;
@@ -675,21 +675,26 @@ g2p_kernel(Ctx ctx, Tape<R> tp, MpmParticles in, MpmParticles out, int advect) {
         for (int b = 0; b < 3; ++b) {
             if (!st.vy[b]) continue;
             const long long rab = st.ox[a] + st.oy[b];
-            const R wab = w[a][0] * w[b][1];
+            // column sums over z: sum w_c g and sum c w_c g
+            R Zg[3] = {0, 0, 0}, Zc[3] = {0, 0, 0};
 #pragma unroll
             for (int c = 0; c < 3; ++c) {
                 if (!st.vz[c]) continue;
                 R g[4];
                 load_node(dense, rab + st.oz[c], g);
-                const R wt = wab * w[c][2];
 #pragma unroll
                 for (int i = 0; i < 3; ++i) {
-                    const R wg = wt * g[1 + i];
-                    nv[i] += wg;
-                    if (a) G[3 * i + 0] += R(a) * wg;
-                    if (b) G[3 * i + 1] += R(b) * wg;
-                    if (c) G[3 * i + 2] += R(c) * wg;
+                    Zg[i] += w[c][2] * g[1 + i];
+                    if (c) Zc[i] += (R(c) * w[c][2]) * g[1 + i];
                 }
+            }
+            const R wab = w[a][0] * w[b][1];
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                nv[i] += wab * Zg[i];
+                if (a) G[3 * i + 0] += (R(a) * wab) * Zg[i];
+                if (b) G[3 * i + 1] += (R(b) * wab) * Zg[i];
+                G[3 * i + 2] += wab * Zc[i];
             }
         }
     }

@@ -94,13 +94,14 @@ typedef struct MpmCotangents {
 
 /* Schedule knobs (picked by the autotuner; zeros select the defaults). */
 typedef struct MpmTuning {
-    int32_t tile_xy;             /* node tile edge in x and y: 4, 8 or 16 (z is fixed at 14) */
+    int32_t tile_xy;             /* node tile edge in x and y: 4, 8 or 16 (default 4)       */
     int32_t scatter_ctas_per_sm; /* persistent P2G node-gather grid = SMs x this (1024-thread CTAs, default 1) */
     int32_t scatter_oxb;         /* stencil x-offsets per pass: 3 (FP32 default) or 1       */
     int32_t particle_block;      /* threads per block of the per-particle kernels: 64, 128 or 256 (default) */
     int32_t active_tile_cap;     /* capacity of the active-tile list (0 = every tile)       */
     float fp64_gap_thresh;       /* FP32 Hencky: relative singular-value gap below this is
                                     recomputed in FP64 (0 selects 1e-6; <0 disables)        */
+    int32_t tile_z;              /* node tile edge in z: 4, 8 or 16 (default 4)             */
 } MpmTuning;
 
 typedef struct MpmPlan MpmPlan;   /* host-side plan (offsets, tile tables)         */

@@ -55,7 +55,8 @@ class MpmCotangents(C.Structure):
 
 class MpmTuning(C.Structure):
     _fields_ = [("tile_xy", i32), ("scatter_ctas_per_sm", i32), ("scatter_oxb", i32),
-                ("particle_block", i32), ("active_tile_cap", i32), ("fp64_gap_thresh", f32)]
+                ("particle_block", i32), ("active_tile_cap", i32), ("fp64_gap_thresh", f32),
+                ("tile_z", i32)]
 
 
 EXPORTS = {

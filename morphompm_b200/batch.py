@@ -162,7 +162,8 @@ class Batch:
 # autotuner
 # ---------------------------------------------------------------------------
 CANDIDATES = {
-    "tile_xy": [4, 8, 16],
+    "tile_xy": [4, 8],
+    "tile_z": [4, 8, 16],
     "scatter_ctas_per_sm": [1, 2],
     "scatter_oxb": [1, 3],
     "particle_block": [128, 256],
@@ -195,7 +196,7 @@ def autotune(scenes: List[dict], dtype=torch.float32, steps: int = 4, budget_s: 
     return the fastest.  Results are deterministic whatever the schedule
     (the summation order per node does not depend on it)."""
     t_start = time.time()
-    best = {"tile_xy": 8, "scatter_ctas_per_sm": 1, "scatter_oxb": 3 if dtype == torch.float32 else 1,
+    best = {"tile_xy": 4, "tile_z": 4, "scatter_ctas_per_sm": 1, "scatter_oxb": 3 if dtype == torch.float32 else 1,
             "particle_block": 256}
     slab = torch.as_tensor(host_slab(scenes, np.float32 if dtype == torch.float32 else np.float64))
 

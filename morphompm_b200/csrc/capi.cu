@@ -5,6 +5,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <climits>
 #include <cstring>
 #include <new>
 #include <vector>
@@ -45,15 +46,15 @@ struct MpmPlan {
     int TN = 0, active_cap = 0;
     bool any_growth = false;
     // workspace offsets
-    size_t o_scenes, o_aux, o_scene_of, o_tile_scene, o_status, o_cell_seg, o_seg_first, o_seg_last, o_blk;
+    size_t o_scenes, o_aux, o_scene_of, o_tile_scene, o_status, o_cell_seg, o_seg_first, o_seg_last, o_blk, o_tblk;
     size_t o_tile_flag, o_keys, o_kalt0, o_valt0, o_kalt1, o_valt1, o_hist, o_totals, o_payload, o_sums;
     size_t o_dense_f = 0, o_dense_b = 0;
     long long n_nodes = 0;
     size_t o_dbuf, o_tape;
-    int nblk_seg = 1;
+    int nblk_seg = 1, nblk_tile = 1;
     size_t ws_bytes = 0;
     // tape offsets
-    size_t t_skeys, t_perm, t_slot, t_active, t_nact, t_grid, tape_bytes = 0;
+    size_t t_skeys, t_perm, t_active, t_nact, t_grid, tape_bytes = 0;
     char* ws = nullptr;
     const void* phi = nullptr;
     int n_sm = 148;
@@ -91,6 +92,7 @@ Ctx make_ctx(MpmPlan* P) {
     c.n_tiles = P->n_tiles;
     c.n_scenes = (int)P->scenes.size();
     c.tile_xy = P->tune.tile_xy;
+    c.tile_z = P->tune.tile_z;
     c.active_cap = P->active_cap;
     c.gap_thresh = P->tune.fp64_gap_thresh < 0 ? 0.0f : P->tune.fp64_gap_thresh;
     return c;
@@ -101,7 +103,6 @@ Tape<R> make_tape(MpmPlan* P, char* t) {
     Tape<R> tp;
     tp.skeys = reinterpret_cast<unsigned*>(t + P->t_skeys);
     tp.perm = reinterpret_cast<unsigned*>(t + P->t_perm);
-    tp.tile_slot = reinterpret_cast<int*>(t + P->t_slot);
     tp.active = reinterpret_cast<int*>(t + P->t_active);
     tp.n_active = reinterpret_cast<int*>(t + P->t_nact);
     tp.grid = reinterpret_cast<R*>(t + P->t_grid);
@@ -148,7 +149,7 @@ inline int check_launch() {
 int build_segments(MpmPlan* P, const Ctx& ctx, const unsigned* skeys, int flag_tiles, cudaStream_t st) {
     Site site(P, MPM_K_MARK, 3, st);
     seg_count_kernel<<<P->nblk_seg, SEG_THREADS, 0, st>>>(ctx, skeys, flag_tiles);
-    seg_scan_kernel<<<1, 1024, 0, st>>>(ctx, P->nblk_seg);
+    scan_counts_kernel<<<1, 1024, 0, st>>>(ctx.blk_count, P->nblk_seg, ctx.n_seg, INT_MAX, ctx.status);
     seg_write_kernel<<<P->nblk_seg, SEG_THREADS, 0, st>>>(ctx, skeys);
     return check_launch();
 }
@@ -161,11 +162,17 @@ void* sums_fn(int oxb) {
     return (void*)cell_sums_kernel<R, MODE, 1>;
 }
 
+template <typename R, int T, int MODE>
+void* nodes_fn_z(int TZ) {
+    if (TZ == 8) return (void*)node_sums_kernel<R, T, 8, MODE>;
+    if (TZ == 16) return (void*)node_sums_kernel<R, T, 16, MODE>;
+    return (void*)node_sums_kernel<R, T, 4, MODE>;
+}
 template <typename R, int MODE>
-void* nodes_fn(int T) {
-    if (T == 4) return (void*)node_sums_kernel<R, 4, MODE>;
-    if (T == 16) return (void*)node_sums_kernel<R, 16, MODE>;
-    return (void*)node_sums_kernel<R, 8, MODE>;
+void* nodes_fn(int T, int TZ) {
+    if (T == 8) return nodes_fn_z<R, 8, MODE>(TZ);
+    if (T == 16) return nodes_fn_z<R, 16, MODE>(TZ);
+    return nodes_fn_z<R, 4, MODE>(TZ);
 }
 
 // P2G phase 2 (node gather + grid epilogue) over the active tiles
@@ -176,7 +183,8 @@ int launch_nodes(MpmPlan* P, int mode, const Ctx& ctx, const int* active, const 
     long long cap = P->n;
     int ctas = P->n_sm * std::max(1, P->tune.scatter_ctas_per_sm);
     ctas = std::max(1, std::min(ctas, P->active_cap));
-    void* f2 = mode == 0 ? nodes_fn<R, 0>(P->tune.tile_xy) : nodes_fn<R, 1>(P->tune.tile_xy);
+    void* f2 = mode == 0 ? nodes_fn<R, 0>(P->tune.tile_xy, P->tune.tile_z)
+                         : nodes_fn<R, 1>(P->tune.tile_xy, P->tune.tile_z);
     void* a2[] = {(void*)&ctx, (void*)&Sc, (void*)&cap, (void*)&active, (void*)&nact, (void*)&grid_out,
                   (void*)&grid_fwd, (void*)&advect};
     return cudaLaunchKernel(f2, dim3(ctas), dim3(1024), a2, 0, st) == cudaSuccess ? MPM_OK : MPM_ERR_CUDA;
@@ -221,8 +229,8 @@ int run_sort(MpmPlan* P, const unsigned* keys, unsigned* skeys, unsigned* perm, 
     return check_launch();
 }
 
-template <typename R, int T>
-int step_fwd_T(MpmPlan* P, const MpmParticles& in, MpmParticles& out, int advect, int t, char* tape,
+template <typename R>
+int step_fwd_R(MpmPlan* P, const MpmParticles& in, MpmParticles& out, int advect, int t, char* tape,
                cudaStream_t st) {
     Ctx ctx = make_ctx(P);
     Tape<R> tp = make_tape<R>(P, tape);
@@ -236,9 +244,12 @@ int step_fwd_T(MpmPlan* P, const MpmParticles& in, MpmParticles& out, int advect
     rc = build_segments(P, ctx, tp.skeys, 1, st);
     if (rc) return rc;
     {
-        Site s(P, MPM_K_COMPACT, 1, st);
-        compact_tiles_kernel<<<1, 1024, 0, st>>>(ctx.tile_flag, P->n_tiles, tp.tile_slot, tp.active, tp.n_active,
-                                                 P->active_cap, ctx.status);
+        Site s(P, MPM_K_COMPACT, 3, st);
+        unsigned* tblk = at<unsigned>(P, P->o_tblk);
+        tile_count_kernel<<<P->nblk_tile, SEG_THREADS, 0, st>>>(ctx.tile_flag, P->n_tiles, tblk);
+        scan_counts_kernel<<<1, 1024, 0, st>>>(tblk, P->nblk_tile, tp.n_active, P->active_cap, ctx.status);
+        tile_write_kernel<<<P->nblk_tile, SEG_THREADS, 0, st>>>(ctx.tile_flag, P->n_tiles, tblk, tp.active,
+                                                                P->active_cap);
     }
     { Site s(P, MPM_K_PREPASS, 1, st); prepass_kernel<R><<<g, B, 0, st>>>(ctx, in, tp.perm, payload, t); }
     rc = check_launch();
@@ -248,12 +259,12 @@ int step_fwd_T(MpmPlan* P, const MpmParticles& in, MpmParticles& out, int advect
         rc = launch_p2g<R>(P, 0, ctx, payload, tp.active, tp.n_active, tp.grid, nullptr, advect, st);
     }
     if (rc) return rc;
-    { Site s(P, MPM_K_G2P, 1, st); g2p_kernel<R, T><<<g, B, 0, st>>>(ctx, tp, in, out, advect); }
+    { Site s(P, MPM_K_G2P, 1, st); g2p_kernel<R><<<g, B, 0, st>>>(ctx, tp, in, out, advect); }
     return check_launch();
 }
 
-template <typename R, int T>
-int step_bwd_T(MpmPlan* P, const MpmParticles& in, const void* outC, const MpmCotangents& ob, MpmCotangents& ib,
+template <typename R>
+int step_bwd_R(MpmPlan* P, const MpmParticles& in, const void* outC, const MpmCotangents& ob, MpmCotangents& ib,
                double* growth_grad, int advect, int t, const char* tape, cudaStream_t st) {
     Ctx ctx = make_ctx(P);
     Tape<R> tp = make_tape<R>(P, const_cast<char*>(tape));
@@ -280,7 +291,7 @@ int step_bwd_T(MpmPlan* P, const MpmParticles& in, const void* outC, const MpmCo
     bool want_dA = growth_grad != nullptr && P->any_growth;
     {
         Site s(P, MPM_K_BWD_PARTICLE, 1, st);
-        bwd_particle_kernel<R, T><<<g, B, 0, st>>>(ctx, tp, in, static_cast<const R*>(outC), ob, ib,
+        bwd_particle_kernel<R><<<g, B, 0, st>>>(ctx, tp, in, static_cast<const R*>(outC), ob, ib,
                                                    want_dA ? dbuf : nullptr, advect, t);
     }
     if (want_dA) {
@@ -288,25 +299,6 @@ int step_bwd_T(MpmPlan* P, const MpmParticles& in, const void* outC, const MpmCo
         scene_reduce_kernel<<<(int)P->scenes.size(), 256, 0, st>>>(ctx, dbuf, growth_grad, 1, 0);
     }
     return check_launch();
-}
-
-template <typename R>
-int step_fwd_R(MpmPlan* P, const MpmParticles& in, MpmParticles& out, int advect, int t, char* tape,
-               cudaStream_t st) {
-    switch (P->tune.tile_xy) {
-        case 4: return step_fwd_T<R, 4>(P, in, out, advect, t, tape, st);
-        case 16: return step_fwd_T<R, 16>(P, in, out, advect, t, tape, st);
-        default: return step_fwd_T<R, 8>(P, in, out, advect, t, tape, st);
-    }
-}
-template <typename R>
-int step_bwd_R(MpmPlan* P, const MpmParticles& in, const void* outC, const MpmCotangents& ob, MpmCotangents& ib,
-               double* gg, int advect, int t, const char* tape, cudaStream_t st) {
-    switch (P->tune.tile_xy) {
-        case 4: return step_bwd_T<R, 4>(P, in, outC, ob, ib, gg, advect, t, tape, st);
-        case 16: return step_bwd_T<R, 16>(P, in, outC, ob, ib, gg, advect, t, tape, st);
-        default: return step_bwd_T<R, 8>(P, in, outC, ob, ib, gg, advect, t, tape, st);
-    }
 }
 
 bool scene_ok(const MpmScene& s) {
@@ -331,15 +323,16 @@ int mpm_plan_create(const MpmScene* scenes, int32_t n_scenes, int32_t real_bytes
     if (!P) return MPM_ERR_ARG;
     P->real_bytes = real_bytes;
     if (tuning) P->tune = *tuning;
-    if (P->tune.tile_xy != 4 && P->tune.tile_xy != 16) P->tune.tile_xy = 8;
+    if (P->tune.tile_xy != 8 && P->tune.tile_xy != 16) P->tune.tile_xy = 4;
+    if (P->tune.tile_z != 8 && P->tune.tile_z != 16) P->tune.tile_z = 4;
     if (P->tune.scatter_ctas_per_sm <= 0) P->tune.scatter_ctas_per_sm = 1;
     if (P->tune.scatter_oxb != 1 && P->tune.scatter_oxb != 3) P->tune.scatter_oxb = real_bytes == 4 ? 3 : 1;
     if (real_bytes == 8) P->tune.scatter_oxb = 1;
     // the per-particle kernels are compiled for at most 256 threads per block
     if (P->tune.particle_block != 64 && P->tune.particle_block != 128) P->tune.particle_block = 256;
     if (P->tune.fp64_gap_thresh == 0.0f) P->tune.fp64_gap_thresh = 1e-6f;
-    const int T = P->tune.tile_xy;
-    P->TN = T * T * TILE_Z;
+    const int T = P->tune.tile_xy, TZ = P->tune.tile_z;
+    P->TN = T * T * TZ;
     long long cell = 0, tile = 0, pcur = 0, nodes = 0;
     for (int s = 0; s < n_scenes; ++s) {
         const MpmScene& sc = scenes[s];
@@ -350,7 +343,7 @@ int mpm_plan_create(const MpmScene* scenes, int32_t n_scenes, int32_t real_bytes
         a.ncells = (sc.shape[0] + 2) * (sc.shape[1] + 2) * (sc.shape[2] + 2);
         a.ntile[0] = (sc.shape[0] + T - 1) / T;
         a.ntile[1] = (sc.shape[1] + T - 1) / T;
-        a.ntile[2] = (sc.shape[2] + TILE_Z - 1) / TILE_Z;
+        a.ntile[2] = (sc.shape[2] + TZ - 1) / TZ;
         a.tile_begin = tile;
         a.node_begin = nodes;
         nodes += (long long)sc.shape[0] * sc.shape[1] * sc.shape[2];
@@ -379,7 +372,6 @@ int mpm_plan_create(const MpmScene* scenes, int32_t n_scenes, int32_t real_bytes
     Layout tl;
     P->t_skeys = tl.take(n * 4);
     P->t_perm = tl.take(n * 4);
-    P->t_slot = tl.take(nt * 4);
     P->t_active = tl.take((size_t)P->active_cap * 4);
     P->t_nact = tl.take(4);
     P->t_grid = tl.take((size_t)P->active_cap * P->TN * 4 * R);
@@ -396,6 +388,8 @@ int mpm_plan_create(const MpmScene* scenes, int32_t n_scenes, int32_t real_bytes
     P->o_seg_first = L.take(n * 4);
     P->o_seg_last = L.take(n * 4);
     P->o_blk = L.take((size_t)P->nblk_seg * 4);
+    P->nblk_tile = (int)((P->n_tiles + SEG_TILE - 1) / SEG_TILE);
+    P->o_tblk = L.take((size_t)P->nblk_tile * 4);
     P->o_tile_flag = L.take(nt * 4);
     P->o_keys = L.take(n * 4);
     P->o_kalt0 = L.take(n * 4);
@@ -679,20 +673,21 @@ int noalloc_scratch(void** out, int* n_sm) {
 // on a plan object that owns no heap memory.
 bool noalloc_layout(MpmPlan& P, const MpmScene& sc, int real_bytes, SceneAux& a) {
     P.real_bytes = real_bytes;
-    P.tune.tile_xy = 8;
+    P.tune.tile_xy = 4;
+    P.tune.tile_z = 4;
     P.tune.scatter_ctas_per_sm = 1;
     P.tune.scatter_oxb = real_bytes == 4 ? 3 : 1;
     P.tune.particle_block = 256;
     P.tune.fp64_gap_thresh = 1e-6f;
-    const int T = P.tune.tile_xy;
-    P.TN = T * T * TILE_Z;
+    const int T = P.tune.tile_xy, TZ = P.tune.tile_z;
+    P.TN = T * T * TZ;
     a.cell_begin = 0;
     a.tile_begin = 0;
     a.node_begin = 0;
     a.ncells = (sc.shape[0] + 2) * (sc.shape[1] + 2) * (sc.shape[2] + 2);
     a.ntile[0] = (sc.shape[0] + T - 1) / T;
     a.ntile[1] = (sc.shape[1] + T - 1) / T;
-    a.ntile[2] = (sc.shape[2] + TILE_Z - 1) / TILE_Z;
+    a.ntile[2] = (sc.shape[2] + TZ - 1) / TZ;
     P.n = sc.p_end;
     P.n_tiles = (long long)a.ntile[0] * a.ntile[1] * a.ntile[2];
     P.n_keys = (long long)a.ncells + 1;
@@ -709,7 +704,6 @@ bool noalloc_layout(MpmPlan& P, const MpmScene& sc, int real_bytes, SceneAux& a)
     Layout tl;
     P.t_skeys = tl.take(n * 4);
     P.t_perm = tl.take(n * 4);
-    P.t_slot = tl.take(nt * 4);
     P.t_active = tl.take((size_t)P.active_cap * 4);
     P.t_nact = tl.take(4);
     P.t_grid = tl.take((size_t)P.active_cap * P.TN * 4 * R);
@@ -724,6 +718,8 @@ bool noalloc_layout(MpmPlan& P, const MpmScene& sc, int real_bytes, SceneAux& a)
     P.o_seg_first = L.take(n * 4);
     P.o_seg_last = L.take(n * 4);
     P.o_blk = L.take((size_t)P.nblk_seg * 4);
+    P.nblk_tile = (int)((P.n_tiles + SEG_TILE - 1) / SEG_TILE);
+    P.o_tblk = L.take((size_t)P.nblk_tile * 4);
     P.o_tile_flag = L.take(nt * 4);
     P.o_keys = L.take(n * 4);
     P.o_kalt0 = L.take(n * 4);

@@ -12,8 +12,7 @@
 
 namespace mpm {
 
-// Node tiles are TILE_XY x TILE_XY x TILE_Z nodes (z fastest inside a tile).
-constexpr int TILE_Z = 16;
+// Node tiles are tile_xy x tile_xy x tile_z nodes (z fastest inside a tile).
 
 // Per-scene data derived on the host from MpmScene.
 struct SceneAux {
@@ -45,6 +44,7 @@ struct Ctx {
     long long n_tiles;
     int n_scenes;
     int tile_xy;
+    int tile_z;
     int active_cap;              // capacity of a tape's active-tile list
     float gap_thresh;            // FP32 Hencky FP64-fallback threshold (relative sv gap)
 };
@@ -55,7 +55,6 @@ template <typename R>
 struct Tape {
     unsigned* skeys;    // sorted cell keys
     unsigned* perm;     // sorted slot -> particle index
-    int* tile_slot;     // dense tile -> slot in the active list (-1 inactive)
     int* active;        // active tile ids
     int* n_active;      // number of active tiles
     R* grid;            // forward node records (m, v0, v1, v2) per slot*TN + local

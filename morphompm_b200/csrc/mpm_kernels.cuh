@@ -186,7 +186,7 @@ __device__ __forceinline__ void flag_tiles(const Ctx& ctx, long long s, unsigned
     int cell[3];
     decode_cell(sc, (long long)k - ax.cell_begin, cell);
     int tlo[3], thi[3];
-    const int T[3] = {ctx.tile_xy, ctx.tile_xy, TILE_Z};
+    const int T[3] = {ctx.tile_xy, ctx.tile_xy, ctx.tile_z};
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
         int b = cell[d] - 2;
@@ -228,16 +228,17 @@ seg_count_kernel(Ctx ctx, const unsigned* __restrict__ skeys, int flag) {
     }
 }
 
-// exclusive scan of the block counts in place; total -> *n_seg (single block)
+// exclusive scan of per-block counts in place (single block); the total,
+// clamped to cap, goes to *total (a total above cap raises MPM_ERR_ARG)
 __global__ void __launch_bounds__(1024)
-seg_scan_kernel(Ctx ctx, int nblk) {
+scan_counts_kernel(unsigned* __restrict__ cnt, int nblk, int* __restrict__ total, int cap, int* __restrict__ status) {
     __shared__ unsigned sh[1024];
     __shared__ unsigned carry;
     if (threadIdx.x == 0) carry = 0;
     __syncthreads();
     for (int b0 = 0; b0 < nblk; b0 += 1024) {
         int b = b0 + threadIdx.x;
-        unsigned v = b < nblk ? ctx.blk_count[b] : 0u;
+        unsigned v = b < nblk ? cnt[b] : 0u;
         sh[threadIdx.x] = v;
         __syncthreads();
         for (int o = 1; o < 1024; o <<= 1) {
@@ -247,12 +248,75 @@ seg_scan_kernel(Ctx ctx, int nblk) {
             __syncthreads();
         }
         unsigned c = carry;
-        if (b < nblk) ctx.blk_count[b] = c + sh[threadIdx.x] - v;
+        if (b < nblk) cnt[b] = c + sh[threadIdx.x] - v;
         __syncthreads();
         if (threadIdx.x == 1023) carry = c + sh[1023];
         __syncthreads();
     }
-    if (threadIdx.x == 0) *ctx.n_seg = (int)carry;
+    if (threadIdx.x == 0) {
+        unsigned c = carry;
+        if (c > (unsigned)cap) {
+            raise_status(status, MPM_ERR_ARG);
+            c = (unsigned)cap;
+        }
+        *total = (int)c;
+    }
+}
+
+// Active-tile list: the tiles flagged by the segment count pass, in tile
+// order.  Per-block counts (warp-striped, coalesced), the block scan above,
+// then ranks from warp ballots; the flags are reset for the next step.
+__global__ void __launch_bounds__(SEG_THREADS)
+tile_count_kernel(const int* __restrict__ flag, long long n_tiles, unsigned* __restrict__ blk) {
+    __shared__ unsigned red[SEG_THREADS / 32];
+    const long long base = (long long)blockIdx.x * SEG_TILE;
+    unsigned cnt = 0;
+#pragma unroll 4
+    for (int r = 0; r < SEG_ITEMS; ++r) {
+        const long long t = base + (long long)r * SEG_THREADS + threadIdx.x;
+        if (t >= n_tiles) break;
+        cnt += flag[t] ? 1u : 0u;
+    }
+    for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = cnt;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned t = 0;
+        for (int w = 0; w < SEG_THREADS / 32; ++w) t += red[w];
+        blk[blockIdx.x] = t;
+    }
+}
+
+__global__ void __launch_bounds__(SEG_THREADS)
+tile_write_kernel(int* __restrict__ flag, long long n_tiles, const unsigned* __restrict__ blk,
+                  int* __restrict__ active, int cap) {
+    constexpr int NW = SEG_THREADS / 32;
+    __shared__ unsigned wtot[NW];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const unsigned lt = (1u << lane) - 1u;
+    const long long base = (long long)blockIdx.x * SEG_TILE;
+    unsigned run = blk[blockIdx.x];
+    for (int r = 0; r < SEG_ITEMS; ++r) {
+        const long long t = base + (long long)r * SEG_THREADS + threadIdx.x;
+        const bool on = t < n_tiles && flag[t] != 0;
+        const unsigned ball = __ballot_sync(0xffffffffu, on);
+        if (lane == 0) wtot[warp] = __popc(ball);
+        __syncthreads();
+        unsigned before = run, round = 0;
+#pragma unroll
+        for (int w = 0; w < NW; ++w) {
+            const unsigned c = wtot[w];
+            if (w < warp) before += c;
+            round += c;
+        }
+        before += __popc(ball & lt);
+        if (on) {
+            if (before < (unsigned)cap) active[before] = (int)t;
+            flag[t] = 0;
+        }
+        run += round;
+        __syncthreads();
+    }
 }
 
 __global__ void __launch_bounds__(SEG_THREADS)
@@ -516,9 +580,9 @@ cell_sums_adj_kernel(Ctx ctx, const unsigned* __restrict__ perm, MpmParticles in
 }
 
 // ---------------------------------------------------------------------------
-// P2G, phase 2: node gather + grid update.  One CTA per active node tile
-// (persistent over the active list); every node adds the sums of its 27
-// source cells in the fixed order o = 0..26, then
+// P2G, phase 2: node gather + grid update.  One thread per node of the
+// active node tiles (persistent grid over the active list); every node adds
+// the sums of its 27 source cells in the fixed order o = 0..26, then
 // MODE 0: grid update -> (m, v[3]) with v = s mom/m + s dt g on free nodes;
 // MODE 1: grid adjoint -> (gm_b, gmom_b[3]) from gv_b and the forward record.
 // ---------------------------------------------------------------------------
@@ -534,14 +598,17 @@ __device__ __forceinline__ void load_sum(const R* __restrict__ S, long long idx,
     }
 }
 
-template <typename R, int T, int MODE>
+template <typename R, int T, int TZ, int MODE>
 __global__ void __launch_bounds__(1024)
 node_sums_kernel(Ctx ctx, const R* __restrict__ S, long long cap, const int* __restrict__ active,
                  const int* __restrict__ n_active, R* __restrict__ grid_out, const R* __restrict__ grid_fwd,
                  int advect) {
-    constexpr int TN = T * T * TILE_Z;
-    const int nact = *n_active;
-    for (int it = blockIdx.x; it < nact; it += gridDim.x) {
+    constexpr int TN = T * T * TZ;
+    // one thread per node of the active tiles (tile-major, z fastest), grid-strided
+    const long long total = (long long)(*n_active) * TN;
+    for (long long gidx = (long long)blockIdx.x * blockDim.x + threadIdx.x; gidx < total;
+         gidx += (long long)gridDim.x * blockDim.x) {
+        const int it = (int)(gidx / TN), node = (int)(gidx % TN);
         const int tile = active[it];
         const int s = ctx.tile_scene[tile];
         const MpmScene& sc = ctx.scenes[s];
@@ -550,14 +617,14 @@ node_sums_kernel(Ctx ctx, const R* __restrict__ S, long long cap, const int* __r
         const int tz = (int)(lt % ax.ntile[2]);
         const int ty = (int)((lt / ax.ntile[2]) % ax.ntile[1]);
         const int tx = (int)(lt / ((long long)ax.ntile[2] * ax.ntile[1]));
-        const int L0 = tx * T, L1 = ty * T, L2 = tz * TILE_Z;
+        const int L0 = tx * T, L1 = ty * T, L2 = tz * TZ;
         const long long P1 = sc.shape[1] + 2, P2 = sc.shape[2] + 2;
         const R s_damp = (R)(1.0 - sc.damping);
         const R dt = (R)sc.dt;
         const R eps = (R)sc.mass_eps;
         const R g0 = (R)sc.gravity[0], g1 = (R)sc.gravity[1], g2 = (R)sc.gravity[2];
-        for (int node = threadIdx.x; node < TN; node += blockDim.x) {
-            const int nz = node % TILE_Z, ny = (node / TILE_Z) % T, nx = node / (TILE_Z * T);
+        {
+            const int nz = node % TZ, ny = (node / TZ) % T, nx = node / (TZ * T);
             const int i = L0 + nx, j = L1 + ny, k = L2 + nz;
             if (i >= sc.shape[0] || j >= sc.shape[1] || k >= sc.shape[2]) continue;
             R acc[4] = {R(0), R(0), R(0), R(0)};
@@ -575,7 +642,6 @@ node_sums_kernel(Ctx ctx, const R* __restrict__ S, long long cap, const int* __r
                             acc[0] += v[0]; acc[1] += v[1]; acc[2] += v[2]; acc[3] += v[3];
                         }
                     }
-            const long long gidx = (long long)it * TN + node;
             const long long didx = ax.node_begin + ((long long)i * sc.shape[1] + j) * sc.shape[2] + k;
             R rec[4] = {R(0), R(0), R(0), R(0)};
             if constexpr (MODE == 0) {
@@ -645,7 +711,7 @@ __device__ __forceinline__ void unmark_cell(const Ctx& ctx, const SceneAux& ax, 
 // G2P + advection + F update (transfer.py:61-79); writes the output state in
 // the input's particle order and clears the cell marks of this step.
 // ---------------------------------------------------------------------------
-template <typename R, int T>
+template <typename R>
 __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 4 : 2)
 g2p_kernel(Ctx ctx, Tape<R> tp, MpmParticles in, MpmParticles out, int advect) {
     long long sidx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -734,7 +800,7 @@ g2p_kernel(Ctx ctx, Tape<R> tp, MpmParticles in, MpmParticles out, int advect) {
 // with M1 = k4 Cn_b'^T, M2 = pm C^T + dt sk^T, and the weight-only terms are
 // summed once per particle: x_b -= M1 sum(w gv) + M2 sum(w mb).
 // ---------------------------------------------------------------------------
-template <typename R, int T>
+template <typename R>
 __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 2 : 1)
 bwd_particle_kernel(Ctx ctx, Tape<R> tp, MpmParticles in, const R* __restrict__ outC,
                     MpmCotangents ob, MpmCotangents ib, double* __restrict__ dA, int advect, int t) {

@@ -144,45 +144,4 @@ radix_scatter_kernel(const unsigned* __restrict__ keys_in, const unsigned* __res
     }
 }
 
-// Tile-list compaction, single block: tile_slot[t] = rank among flagged tiles
-// (or -1), active[rank] = t, *n_active = count.  Flags are reset to 0.
-__global__ void __launch_bounds__(1024)
-compact_tiles_kernel(int* __restrict__ flag, long long n_tiles, int* __restrict__ tile_slot,
-                     int* __restrict__ active, int* __restrict__ n_active, int cap, int* __restrict__ status) {
-    __shared__ int sh[1024];
-    long long per = (n_tiles + 1023) / 1024;
-    long long t0 = (long long)threadIdx.x * per;
-    long long t1 = t0 + per < n_tiles ? t0 + per : n_tiles;
-    int cnt = 0;
-    for (long long t = t0; t < t1; ++t) cnt += flag[t] ? 1 : 0;
-    sh[threadIdx.x] = cnt;
-    __syncthreads();
-    for (int o = 1; o < 1024; o <<= 1) {
-        int v = (threadIdx.x >= (unsigned)o) ? sh[threadIdx.x - o] : 0;
-        __syncthreads();
-        sh[threadIdx.x] += v;
-        __syncthreads();
-    }
-    int run = sh[threadIdx.x] - cnt;
-    for (long long t = t0; t < t1; ++t) {
-        if (flag[t]) {
-            if (run < cap) {
-                tile_slot[t] = run;
-                active[run] = (int)t;
-            } else {
-                tile_slot[t] = -1;
-            }
-            ++run;
-            flag[t] = 0;
-        } else {
-            tile_slot[t] = -1;
-        }
-    }
-    if (threadIdx.x == 1023) {
-        int total = sh[1023];
-        if (total > cap) { atomicOr(status, MPM_ERR_ARG); total = cap; }
-        *n_active = total;
-    }
-}
-
 }  // namespace mpm

@@ -96,6 +96,7 @@ def tuning_struct(t: Optional[dict]) -> L.MpmTuning:
     c.particle_block = int(t.get("particle_block", 0))
     c.active_tile_cap = int(t.get("active_tile_cap", 0))
     c.fp64_gap_thresh = float(t.get("fp64_gap_thresh", 0.0))
+    c.tile_z = int(t.get("tile_z", 0))
     return c
 
 

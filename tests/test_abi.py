@@ -44,7 +44,7 @@ int main(void) {
          sizeof(MpmParticles), sizeof(MpmCotangents), sizeof(MpmTuning));
   O(MpmScene, p_begin); O(MpmScene, wall); O(MpmScene, growth_mode); O(MpmScene, dx); O(MpmScene, gravity);
   O(MpmScene, mu); O(MpmScene, kappa); O(MpmScene, eps); O(MpmScene, growth_A); O(MpmScene, ramp_steps);
-  O(MpmParticles, Fg); O(MpmParticles, sc9); O(MpmCotangents, Fg); O(MpmTuning, fp64_gap_thresh);
+  O(MpmParticles, Fg); O(MpmParticles, sc9); O(MpmCotangents, Fg); O(MpmTuning, fp64_gap_thresh); O(MpmTuning, tile_z);
   return 0;
 }
 '''

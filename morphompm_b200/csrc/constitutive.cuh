@@ -400,7 +400,7 @@ __device__ __forceinline__ void hb_vjp(const R F[9], const R Fg[9], const R C[9]
 // went to FP64 and the VJP must do the same.
 // ---------------------------------------------------------------------------
 template <typename R>
-__device__ __noinline__ bool hencky_stress_keep(const R* F, const R* Fg, R mu, R lam, float thresh, R* tau,
+__device__ __forceinline__ bool hencky_stress_keep(const R* F, const R* Fg, R mu, R lam, float thresh, R* tau,
                                                 R* keep) {
     R Fgi[9], Fe[9], beta[3], V[9];
     hencky_eig(F, Fg, Fgi, Fe, beta, V);
@@ -419,7 +419,7 @@ __device__ __noinline__ bool hencky_stress_keep(const R* F, const R* Fg, R mu, R
     return fp64;
 }
 template <typename R>
-__device__ __noinline__ bool hencky_vjp_keep(const R* F, const R* Fg, R mu, R lam, float thresh, const R* tb,
+__device__ __forceinline__ bool hencky_vjp_keep(const R* F, const R* Fg, R mu, R lam, float thresh, const R* tb,
                                              const R* keep, R* Fb, R* Fgb) {
     if (keep[12] != R(0)) return Hencky<R>::vjp(F, Fg, mu, lam, thresh, tb, Fb, Fgb);
     R Fgi[9], Fe[9], beta[3], V[9];
@@ -435,9 +435,11 @@ __device__ __noinline__ bool hencky_vjp_keep(const R* F, const R* Fg, R mu, R la
 
 // ---------------------------------------------------------------------------
 // model dispatch.  Returns true when an FP32 Hencky evaluation went to FP64.
-// Hencky and Herschel-Bulkley are called out of line so that their register
-// demand (the eigensolve, the FP64 recompute) does not inflate the register
-// allocation of the kernels that fuse them.
+// The stand-alone Hencky stress and VJP are called out of line so that their
+// register demand (the eigensolve, the FP64 recompute) does not inflate the
+// allocation of the kernels that fuse them; the reverse kernel's variants that
+// keep the eigendecomposition are inlined (out-of-line calls would pass their
+// arrays through the local-memory stack).
 // ---------------------------------------------------------------------------
 template <typename R>
 __device__ __noinline__ bool hencky_stress_ool(const R* F, const R* Fg, R mu, R lam, float thresh, R* tau) {
@@ -449,27 +451,17 @@ __device__ __noinline__ bool hencky_vjp_ool(const R* F, const R* Fg, R mu, R lam
     return Hencky<R>::vjp(F, Fg, mu, lam, thresh, tb, Fb, Fgb);
 }
 template <typename R>
-__device__ __noinline__ void hb_stress_ool(const R* F, const R* Fg, const R* C, const ModelParams<R> P, R* tau) {
-    hb_stress(F, Fg, C, P, tau);
-}
-template <typename R>
-__device__ __noinline__ void hb_vjp_ool(const R* F, const R* Fg, const R* C, const ModelParams<R> P, const R* tb,
-                                        R* Fb, R* Fgb, R* Cb) {
-    hb_vjp(F, Fg, C, P, tb, Fb, Fgb, Cb);
-}
-
-template <typename R>
 __device__ __forceinline__ bool model_stress(const ModelParams<R>& P, float thresh, const R F[9], const R Fg[9],
                                              const R C[9], R tau[9]) {
     if (P.kind == MPM_MODEL_HENCKY) return hencky_stress_ool<R>(F, Fg, P.mu, P.lam, thresh, tau);
-    if (P.kind == MPM_MODEL_HERSCHEL_BULKLEY) { hb_stress_ool<R>(F, Fg, C, P, tau); return false; }
+    if (P.kind == MPM_MODEL_HERSCHEL_BULKLEY) { hb_stress<R>(F, Fg, C, P, tau); return false; }
     nh_stress(F, Fg, P.mu, P.lam, tau);
     return false;
 }
 template <typename R>
 __device__ __forceinline__ bool model_vjp(const ModelParams<R>& P, float thresh, const R F[9], const R Fg[9],
                                           const R C[9], const R tb[9], R Fb[9], R Fgb[9], R Cb[9]) {
-    if (P.kind == MPM_MODEL_HERSCHEL_BULKLEY) { hb_vjp_ool<R>(F, Fg, C, P, tb, Fb, Fgb, Cb); return false; }
+    if (P.kind == MPM_MODEL_HERSCHEL_BULKLEY) { hb_vjp<R>(F, Fg, C, P, tb, Fb, Fgb, Cb); return false; }
 #pragma unroll
     for (int i = 0; i < 9; ++i) Cb[i] = R(0);
     if (P.kind == MPM_MODEL_HENCKY) return hencky_vjp_ool<R>(F, Fg, P.mu, P.lam, thresh, tb, Fb, Fgb);

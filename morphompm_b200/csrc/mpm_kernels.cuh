@@ -419,6 +419,75 @@ __device__ __forceinline__ void store_sum(R* __restrict__ S, long long idx, cons
     }
 }
 
+// Adds one particle record's contributions to the stencil sums of the x-offsets
+// ox0 .. ox0+OXB-1: w(o) (a + B dp(o)) (and w(o) m in channel 0 for MODE 0),
+// dp = o - fx in cell units (B carries the dx factor).
+template <typename R, int MODE, int OXB>
+__device__ __forceinline__ void accumulate_record(const R r[PAYLOAD], int ox0, R acc[OXB][3][3][4]) {
+    R w[3][3];
+    bspline(r, w);
+    R dz[3] = {R(0) - r[2], R(1) - r[2], R(2) - r[2]};
+    R dy[3] = {R(0) - r[1], R(1) - r[1], R(2) - r[1]};
+#pragma unroll
+    for (int a = 0; a < OXB; ++a) {
+        const int ox = ox0 + a;
+        const R dpx = R(ox) - r[0];
+        R wx;
+        if constexpr (OXB == 3) wx = w[a][0];
+        else wx = ox == 0 ? w[0][0] : (ox == 1 ? w[1][0] : w[2][0]);
+        // a + B dp with dp = (dpx, dy, dz), x part hoisted
+        const R ax0 = r[4] + r[7] * dpx, ax1 = r[5] + r[10] * dpx, ax2 = r[6] + r[13] * dpx;
+#pragma unroll
+        for (int oy = 0; oy < 3; ++oy) {
+            const R wxy = wx * w[oy][1];
+            const R ay0 = ax0 + r[8] * dy[oy], ay1 = ax1 + r[11] * dy[oy], ay2 = ax2 + r[14] * dy[oy];
+#pragma unroll
+            for (int oz = 0; oz < 3; ++oz) {
+                const R wt = wxy * w[oz][2];
+                const R q0 = ay0 + r[9] * dz[oz];
+                const R q1 = ay1 + r[12] * dz[oz];
+                const R q2 = ay2 + r[15] * dz[oz];
+                if constexpr (MODE == 0) {
+                    acc[a][oy][oz][0] += wt * r[3];
+                    acc[a][oy][oz][1] += wt * q0;
+                    acc[a][oy][oz][2] += wt * q1;
+                    acc[a][oy][oz][3] += wt * q2;
+                } else {
+                    acc[a][oy][oz][0] += wt * q0;
+                    acc[a][oy][oz][1] += wt * q1;
+                    acc[a][oy][oz][2] += wt * q2;
+                }
+            }
+        }
+    }
+}
+
+template <typename R, int OXB>
+__device__ __forceinline__ void zero_acc(R acc[OXB][3][3][4]) {
+#pragma unroll
+    for (int a = 0; a < OXB; ++a)
+#pragma unroll
+        for (int b = 0; b < 3; ++b)
+#pragma unroll
+            for (int c = 0; c < 3; ++c)
+#pragma unroll
+                for (int h = 0; h < 4; ++h) acc[a][b][c][h] = R(0);
+}
+
+template <typename R, int OXB>
+__device__ __forceinline__ void store_acc(R* __restrict__ S, long long cap, int id, int ox0,
+                                          R acc[OXB][3][3][4]) {
+#pragma unroll
+    for (int a = 0; a < OXB; ++a)
+#pragma unroll
+        for (int oy = 0; oy < 3; ++oy)
+#pragma unroll
+            for (int oz = 0; oz < 3; ++oz) {
+                const int o = 9 * (ox0 + a) + 3 * oy + oz;
+                store_sum(S, (long long)o * cap + id, acc[a][oy][oz]);
+            }
+}
+
 template <typename R, int MODE, int OXB>
 __global__ void __launch_bounds__(128)
 cell_sums_kernel(Ctx ctx, const R* __restrict__ payload, R* __restrict__ S, long long cap) {
@@ -428,63 +497,13 @@ cell_sums_kernel(Ctx ctx, const R* __restrict__ payload, R* __restrict__ S, long
 #pragma unroll 1
         for (int ox0 = 0; ox0 < 3; ox0 += OXB) {
             R acc[OXB][3][3][4];
-#pragma unroll
-            for (int a = 0; a < OXB; ++a)
-#pragma unroll
-                for (int b = 0; b < 3; ++b)
-#pragma unroll
-                    for (int c = 0; c < 3; ++c)
-#pragma unroll
-                        for (int h = 0; h < 4; ++h) acc[a][b][c][h] = R(0);
+            zero_acc<R, OXB>(acc);
             for (int q = first; q < last; ++q) {
                 R r[PAYLOAD];
                 load_record(payload, q, r);
-                R w[3][3];
-                bspline(r, w);
-                R dz[3] = {R(0) - r[2], R(1) - r[2], R(2) - r[2]};
-                R dy[3] = {R(0) - r[1], R(1) - r[1], R(2) - r[1]};
-#pragma unroll
-                for (int a = 0; a < OXB; ++a) {
-                    const int ox = ox0 + a;
-                    const R dpx = R(ox) - r[0];
-                    R wx;
-                    if constexpr (OXB == 3) wx = w[a][0];
-                    else wx = ox == 0 ? w[0][0] : (ox == 1 ? w[1][0] : w[2][0]);
-                    // a + B dp with dp = (dpx, dy, dz), x part hoisted
-                    const R ax0 = r[4] + r[7] * dpx, ax1 = r[5] + r[10] * dpx, ax2 = r[6] + r[13] * dpx;
-#pragma unroll
-                    for (int oy = 0; oy < 3; ++oy) {
-                        const R wxy = wx * w[oy][1];
-                        const R ay0 = ax0 + r[8] * dy[oy], ay1 = ax1 + r[11] * dy[oy], ay2 = ax2 + r[14] * dy[oy];
-#pragma unroll
-                        for (int oz = 0; oz < 3; ++oz) {
-                            const R wt = wxy * w[oz][2];
-                            const R q0 = ay0 + r[9] * dz[oz];
-                            const R q1 = ay1 + r[12] * dz[oz];
-                            const R q2 = ay2 + r[15] * dz[oz];
-                            if constexpr (MODE == 0) {
-                                acc[a][oy][oz][0] += wt * r[3];
-                                acc[a][oy][oz][1] += wt * q0;
-                                acc[a][oy][oz][2] += wt * q1;
-                                acc[a][oy][oz][3] += wt * q2;
-                            } else {
-                                acc[a][oy][oz][0] += wt * q0;
-                                acc[a][oy][oz][1] += wt * q1;
-                                acc[a][oy][oz][2] += wt * q2;
-                            }
-                        }
-                    }
-                }
+                accumulate_record<R, MODE, OXB>(r, ox0, acc);
             }
-#pragma unroll
-            for (int a = 0; a < OXB; ++a)
-#pragma unroll
-                for (int oy = 0; oy < 3; ++oy)
-#pragma unroll
-                    for (int oz = 0; oz < 3; ++oz) {
-                        const int o = 9 * (ox0 + a) + 3 * oy + oz;
-                        store_sum(S, (long long)o * cap + id, acc[a][oy][oz]);
-                    }
+            store_acc<R, OXB>(S, cap, id, ox0, acc);
         }
     }
 }
@@ -824,6 +843,11 @@ bwd_particle_kernel(Ctx ctx, Tape<R> tp, MpmParticles in, const R* __restrict__ 
 
     R tau[9], keep[13];
     bool fb = model_stress_keep(M, ctx.gap_thresh, F, Fg, C, tau, keep);
+    // the kept eigendecomposition waits in shared memory (one column per
+    // thread) while the node loop holds the registers
+    __shared__ R keep_s[13][256];
+#pragma unroll
+    for (int i = 0; i < 13; ++i) keep_s[i][threadIdx.x] = keep[i];
     const R c = -k4 * (R)sc.vol0 * det3(Fg);
 
     // per-particle matrices of the regrouped x_b terms
@@ -967,6 +991,12 @@ bwd_particle_kernel(Ctx ctx, Tape<R> tp, MpmParticles in, const R* __restrict__ 
         taub[i] = c * skb[i];
     }
     R Fb2[9], Fgb[9], Cb2[9];
+    {
+        // volatile: reload here rather than keep the values live in registers
+        volatile R* ks = &keep_s[0][threadIdx.x];
+#pragma unroll
+        for (int i = 0; i < 13; ++i) keep[i] = ks[i * 256];
+    }
     fb |= model_vjp_keep(M, ctx.gap_thresh, F, Fg, C, taub, keep, Fb2, Fgb, Cb2);
     if (fb) atomicAdd(ctx.fallbacks, 1ull);
 #pragma unroll

@@ -152,6 +152,22 @@ int mpm_plan_set_growth_field(MpmPlan* plan, const void* phi);
 int mpm_step_fwd(MpmPlan* plan, const MpmParticles* in, MpmParticles* out, int32_t advect,
                  int32_t step_index, void* tape, void* stream);
 
+/* Flags of mpm_step_fwd_chain. */
+#define MPM_FWD_CHAINED 1   /* `in` is the `out` of the previous MPM_FWD_EMIT call on this plan */
+#define MPM_FWD_EMIT    2   /* also bin `out` and form its P2G records for step_index + 1 */
+
+/* mpm_step_fwd for consecutive steps of one trajectory.  No counterpart in the
+ * reference, whose step (python/morphompm/transfer.py:33-79) re-derives the
+ * binning and the stress of its input every call.  With MPM_FWD_EMIT the G2P
+ * pass also bins the new state and evaluates its stress (Fg of the growth law
+ * at step_index + 1, or the same explicit Fg); a following call with
+ * MPM_FWD_CHAINED then skips its binning and stress passes.  The results are
+ * those of mpm_step_fwd.  A CHAINED call whose `in` (every pointer and stride)
+ * or step_index does not continue the last EMIT call, or that follows any
+ * other forward call on the plan, returns MPM_ERR_ARG. */
+int mpm_step_fwd_chain(MpmPlan* plan, const MpmParticles* in, MpmParticles* out, int32_t advect,
+                       int32_t step_index, void* tape, int32_t flags, void* stream);
+
 /* Reverse of mpm_step_fwd for the step recorded in `tape`.
  * Replaces python/morphompm/transfer.py:82-158 (step_vjp).
  * `in` is the step's input state, `out_C` the C of its output state.

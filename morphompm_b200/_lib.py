@@ -19,6 +19,8 @@ MPM_WARN_OUTSIDE = 8
 MPM_ERR_TAPE = 16
 MPM_ERR_UNSUPPORTED = 32
 MPM_ERR_TOO_LARGE = 64
+MPM_FWD_CHAINED = 1
+MPM_FWD_EMIT = 2
 
 KERNELS = ["bin", "sort", "mark", "compact", "prepass", "p2g", "g2p", "bwd_payload", "bwd_p2g",
            "bwd_particle", "reduce"]
@@ -75,6 +77,7 @@ EXPORTS = {
     "mpm_plan_launch_count": (i64, [vp]),
     "mpm_plan_active_tiles": (i32, [vp, vp, C.POINTER(i32), vp]),
     "mpm_step_fwd": (i32, [vp, C.POINTER(MpmParticles), C.POINTER(MpmParticles), i32, i32, vp, vp]),
+    "mpm_step_fwd_chain": (i32, [vp, C.POINTER(MpmParticles), C.POINTER(MpmParticles), i32, i32, vp, i32, vp]),
     "mpm_step_bwd": (i32, [vp, C.POINTER(MpmParticles), vp, C.POINTER(MpmCotangents),
                            C.POINTER(MpmCotangents), vp, i32, i32, vp, vp]),
     "mpm_stress": (i32, [C.POINTER(MpmScene), i32, i64, vp, vp, vp, vp, vp]),

@@ -123,7 +123,8 @@ class Batch:
         b = torch.empty_like(a)
         mx = 0
         for t in range(self.n_steps):
-            plan.step_fwd(slab_particles(a), slab_particles(b), advect, t, None)
+            plan.step_fwd(slab_particles(a), slab_particles(b), advect, t, None, chained=t > 0,
+                          emit=t + 1 < self.n_steps)
             mx = max(mx, plan.active_tiles(None))
             a, b = b, a
         return int(1.25 * mx) + 16

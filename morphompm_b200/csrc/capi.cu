@@ -52,6 +52,10 @@ struct MpmPlan {
     long long n_nodes = 0;
     size_t o_dbuf, o_tape;
     int nblk_seg = 1, nblk_tile = 1;
+    // the state whose keys and P2G records the last MPM_FWD_EMIT call formed
+    bool chain_valid = false;
+    int chain_t = 0;
+    MpmParticles chain_state{};
     size_t ws_bytes = 0;
     // tape offsets
     size_t t_skeys, t_perm, t_active, t_nact, t_grid, tape_bytes = 0;
@@ -192,14 +196,15 @@ int launch_nodes(MpmPlan* P, int mode, const Ctx& ctx, const int* active, const 
 
 // two-phase P2G: per-cell stencil sums, then per-node gather + grid epilogue
 template <typename R>
-int launch_p2g(MpmPlan* P, int mode, const Ctx& ctx, const R* payload, const int* active, const int* nact,
+int launch_p2g(MpmPlan* P, int mode, const Ctx& ctx, const unsigned* perm, const R* payload, const int* active,
+               const int* nact,
                R* grid_out, const R* grid_fwd, int advect, cudaStream_t st) {
     R* S = at<R>(P, P->o_sums);
     long long cap = P->n;
     int blocks1 = (int)std::min<long long>((P->n + 127) / 128, (long long)P->n_sm * 16);
     blocks1 = std::max(1, blocks1);
     void* f1 = mode == 0 ? sums_fn<R, 0>(P->tune.scatter_oxb) : sums_fn<R, 1>(P->tune.scatter_oxb);
-    void* a1[] = {(void*)&ctx, (void*)&payload, (void*)&S, (void*)&cap};
+    void* a1[] = {(void*)&ctx, (void*)&perm, (void*)&payload, (void*)&S, (void*)&cap};
     if (cudaLaunchKernel(f1, dim3(blocks1), dim3(128), a1, 0, st) != cudaSuccess) return MPM_ERR_CUDA;
     P->launches += 1;   // the Site around this call counts one
     return launch_nodes<R>(P, mode, ctx, active, nact, grid_out, grid_fwd, advect, st);
@@ -229,16 +234,19 @@ int run_sort(MpmPlan* P, const unsigned* keys, unsigned* skeys, unsigned* perm, 
     return check_launch();
 }
 
+// flags: MPM_FWD_CHAINED (keys and P2G records of `in` already formed by the
+// previous step's G2P), MPM_FWD_EMIT (form them for `out` in this G2P)
 template <typename R>
 int step_fwd_R(MpmPlan* P, const MpmParticles& in, MpmParticles& out, int advect, int t, char* tape,
-               cudaStream_t st) {
+               int flags, cudaStream_t st) {
+    const bool chained = (flags & MPM_FWD_CHAINED) != 0, emit = (flags & MPM_FWD_EMIT) != 0;
     Ctx ctx = make_ctx(P);
     Tape<R> tp = make_tape<R>(P, tape);
     const int B = P->tune.particle_block;
     const int g = grid_for(P->n, B);
     unsigned* keys = at<unsigned>(P, P->o_keys);
     R* payload = at<R>(P, P->o_payload);
-    { Site s(P, MPM_K_BIN, 1, st); bin_kernel<R><<<g, B, 0, st>>>(ctx, in, keys); }
+    if (!chained) { Site s(P, MPM_K_BIN, 1, st); bin_kernel<R><<<g, B, 0, st>>>(ctx, in, keys); }
     int rc = run_sort(P, keys, tp.skeys, tp.perm, st);
     if (rc) return rc;
     rc = build_segments(P, ctx, tp.skeys, 1, st);
@@ -251,15 +259,21 @@ int step_fwd_R(MpmPlan* P, const MpmParticles& in, MpmParticles& out, int advect
         tile_write_kernel<<<P->nblk_tile, SEG_THREADS, 0, st>>>(ctx.tile_flag, P->n_tiles, tblk, tp.active,
                                                                 P->active_cap);
     }
-    { Site s(P, MPM_K_PREPASS, 1, st); prepass_kernel<R><<<g, B, 0, st>>>(ctx, in, tp.perm, payload, t); }
+    if (!chained) { Site s(P, MPM_K_PREPASS, 1, st); prepass_kernel<R><<<g, B, 0, st>>>(ctx, in, payload, t); }
     rc = check_launch();
     if (rc) return rc;
     {
         Site s(P, MPM_K_P2G, 1, st);
-        rc = launch_p2g<R>(P, 0, ctx, payload, tp.active, tp.n_active, tp.grid, nullptr, advect, st);
+        rc = launch_p2g<R>(P, 0, ctx, tp.perm, payload, tp.active, tp.n_active, tp.grid, nullptr, advect, st);
     }
     if (rc) return rc;
-    { Site s(P, MPM_K_G2P, 1, st); g2p_kernel<R><<<g, B, 0, st>>>(ctx, tp, in, out, advect); }
+    {
+        Site s(P, MPM_K_G2P, 1, st);
+        if (emit)
+            g2p_kernel<R, true><<<g, B, 0, st>>>(ctx, tp, in, out, advect, keys, payload, t);
+        else
+            g2p_kernel<R, false><<<g, B, 0, st>>>(ctx, tp, in, out, advect, keys, payload, t);
+    }
     return check_launch();
 }
 
@@ -518,18 +532,36 @@ int mpm_plan_set_growth_field(MpmPlan* P, const void* phi) {
     return MPM_OK;
 }
 
-int mpm_step_fwd(MpmPlan* P, const MpmParticles* in, MpmParticles* out, int32_t advect, int32_t step_index,
-                 void* tape, void* stream) {
+int mpm_step_fwd_chain(MpmPlan* P, const MpmParticles* in, MpmParticles* out, int32_t advect, int32_t step_index,
+                       void* tape, int32_t flags, void* stream) {
     if (!P || !P->ws || !in || !out || !in->x || !in->v || !in->C || !in->F || !out->x || !out->v || !out->C ||
-        !out->F || in->x == out->x || in->F == out->F)
+        !out->F || in->x == out->x || in->F == out->F || (flags & ~(MPM_FWD_CHAINED | MPM_FWD_EMIT)) != 0)
         return MPM_ERR_ARG;
     for (const MpmScene& s : P->scenes)
         if (s.growth_mode == 0 && !in->Fg) return MPM_ERR_ARG;
     char* tp = tape ? static_cast<char*>(tape) : P->ws + P->o_tape;
     if (reinterpret_cast<uintptr_t>(tp) % ALIGN) return MPM_ERR_ARG;
+    // a chained step must continue the last emitting call on this plan
+    if (flags & MPM_FWD_CHAINED) {
+        if (!P->chain_valid || P->chain_t != step_index ||
+            std::memcmp(&P->chain_state, in, sizeof(MpmParticles)) != 0)
+            return MPM_ERR_ARG;
+    }
+    P->chain_valid = false;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    return P->real_bytes == 4 ? step_fwd_R<float>(P, *in, *out, advect, step_index, tp, st)
-                              : step_fwd_R<double>(P, *in, *out, advect, step_index, tp, st);
+    int rc = P->real_bytes == 4 ? step_fwd_R<float>(P, *in, *out, advect, step_index, tp, flags, st)
+                                : step_fwd_R<double>(P, *in, *out, advect, step_index, tp, flags, st);
+    if (rc == MPM_OK && (flags & MPM_FWD_EMIT)) {
+        P->chain_valid = true;
+        P->chain_t = step_index + 1;
+        P->chain_state = *out;
+    }
+    return rc;
+}
+
+int mpm_step_fwd(MpmPlan* P, const MpmParticles* in, MpmParticles* out, int32_t advect, int32_t step_index,
+                 void* tape, void* stream) {
+    return mpm_step_fwd_chain(P, in, out, advect, step_index, tape, 0, stream);
 }
 
 int mpm_step_bwd(MpmPlan* P, const MpmParticles* in, const void* out_C, const MpmCotangents* out_bar,
@@ -765,8 +797,8 @@ extern "C" int mpm_step_fwd_noalloc(const MpmScene* scene, int32_t real_bytes, c
         cudaMemsetAsync(P.ws + P.o_cell_seg, 0, (size_t)P.n_keys * 4, st) != cudaSuccess ||
         cudaMemsetAsync(P.ws + P.o_tile_flag, 0, (size_t)P.n_tiles * 4, st) != cudaSuccess)
         return MPM_ERR_CUDA;
-    rc = real_bytes == 4 ? step_fwd_R<float>(&P, *in, *out, advect, step_index, P.ws + P.o_tape, st)
-                         : step_fwd_R<double>(&P, *in, *out, advect, step_index, P.ws + P.o_tape, st);
+    rc = real_bytes == 4 ? step_fwd_R<float>(&P, *in, *out, advect, step_index, P.ws + P.o_tape, 0, st)
+                         : step_fwd_R<double>(&P, *in, *out, advect, step_index, P.ws + P.o_tape, 0, st);
     if (rc) return rc;
     if (status) {
         if (cudaMemcpyAsync(status, P.ws + P.o_status, 4, cudaMemcpyDeviceToHost, st) != cudaSuccess ||

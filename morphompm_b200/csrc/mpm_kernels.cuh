@@ -5,11 +5,13 @@
 //   radix sort        (sort.cuh) cell-sorted particle order, deterministic
 //   seg_* kernels     segment table of the occupied cells + active tile flags
 //   compact_tiles     active node tiles -> compact grid slots
-//   prepass_kernel    stress and the P2G payload of every particle, sorted order
+//   prepass_kernel    stress and the P2G record of every particle (particle order);
+//                     in a chain of steps the previous G2P forms them instead
 //   cell_sums_kernel  P2G phase 1: per occupied cell, its 27 stencil sums
 //   node_sums_kernel  P2G phase 2: per node, the sums of its 27 source cells
 //                     in a fixed order, + grid update with boundary conditions
-//   g2p_kernel        gather, advect, F update; clears the cell marks
+//   g2p_kernel        gather, advect, F update; clears the cell marks; in a
+//                     chain also bins the new state and forms its P2G records
 // Reverse (python/morphompm/transfer.py:82-158):
 //   cell_sums_adj     gv_b scatter phase 1 (nv_b, Cn_b' formed per particle)
 //   node_sums<1>      gv_b gather + grid adjoint (gmom_b, gm_b)
@@ -114,29 +116,30 @@ __device__ __forceinline__ void load_Fg(const Ctx& ctx, const MpmScene& sc, cons
 // ---------------------------------------------------------------------------
 // binning
 // ---------------------------------------------------------------------------
+// cell key of a particle at x (its padded stencil-base cell, or the scene's
+// "outside" key) and its fractional position fx in the stencil
+template <typename R>
+__device__ __forceinline__ unsigned particle_key(const Ctx& ctx, const MpmScene& sc, const SceneAux& ax,
+                                                 const R x[3], R fx[3]) {
+    int base[3];
+    const bool inside = bin_particle(x, (R)(1.0 / sc.dx), sc.shape, base, fx);
+    if (inside) {
+        long long c = ((long long)(base[0] + 2) * (sc.shape[1] + 2) + (base[1] + 2)) * (sc.shape[2] + 2) + (base[2] + 2);
+        return (unsigned)(ax.cell_begin + c);
+    }
+    raise_status(ctx.status, MPM_WARN_OUTSIDE);
+    return (unsigned)(ax.cell_begin + ax.ncells);
+}
+
 template <typename R>
 __global__ void __launch_bounds__(256)
 bin_kernel(Ctx ctx, MpmParticles P, unsigned* __restrict__ keys) {
     long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= ctx.n) return;
     int s = ctx.scene_of[p];
-    const MpmScene& sc = ctx.scenes[s];
-    const SceneAux& ax = ctx.aux[s];
-    R x[3];
+    R x[3], fx[3];
     ld3<R>(P.x, p, P.sp3, P.sc3, x);
-    R inv_dx = (R)(1.0 / sc.dx);
-    int base[3];
-    R fx[3];
-    bool inside = bin_particle(x, inv_dx, sc.shape, base, fx);
-    unsigned key;
-    if (inside) {
-        long long c = ((long long)(base[0] + 2) * (sc.shape[1] + 2) + (base[1] + 2)) * (sc.shape[2] + 2) + (base[2] + 2);
-        key = (unsigned)(ax.cell_begin + c);
-    } else {
-        key = (unsigned)(ax.cell_begin + ax.ncells);
-        raise_status(ctx.status, MPM_WARN_OUTSIDE);
-    }
-    keys[p] = key;
+    keys[p] = particle_key<R>(ctx, ctx.scenes[s], ctx.aux[s], x, fx);
 }
 
 // keys of a single scene (C ABI mpm_bin_keys); local keys, no plan
@@ -363,24 +366,14 @@ seg_write_kernel(Ctx ctx, const unsigned* __restrict__ skeys) {
 }
 
 // ---------------------------------------------------------------------------
-// forward prepass: stress -> payload record (sorted order)
+// forward prepass: stress -> P2G record, stored in particle order
 // record: fx[0..2], pmass, a = pmass v, B = (pmass C + dt sk) dx
 // ---------------------------------------------------------------------------
 template <typename R>
-__global__ void __launch_bounds__(256, 3)
-prepass_kernel(Ctx ctx, MpmParticles P, const unsigned* __restrict__ perm, R* __restrict__ payload, int t) {
-    long long sidx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (sidx >= ctx.n) return;
-    long long p = perm[sidx];
-    const MpmScene& sc = ctx.scenes[ctx.scene_of[sidx]];
+__device__ __forceinline__ void p2g_record(const Ctx& ctx, const MpmScene& sc, const R fx[3], const R v[3],
+                                           const R C[9], const R F[9], const R Fg[9], R rec[PAYLOAD]) {
     ModelParams<R> M;
     M.load(sc);
-    R x[3], v[3], C[9], F[9], Fg[9];
-    ld3<R>(P.x, p, P.sp3, P.sc3, x);
-    ld3<R>(P.v, p, P.sp3, P.sc3, v);
-    ld9<R>(P.C, p, P.sp9, P.sc9, C);
-    ld9<R>(P.F, p, P.sp9, P.sc9, F);
-    load_Fg<R>(ctx, sc, P, p, t, Fg, nullptr);
     const R dx = (R)sc.dx, dt = (R)sc.dt, inv_dx = (R)(1.0 / sc.dx);
     const R k4 = R(4) * inv_dx * inv_dx;
     R tau[9];
@@ -388,17 +381,32 @@ prepass_kernel(Ctx ctx, MpmParticles P, const unsigned* __restrict__ perm, R* __
     if (fb) atomicAdd(ctx.fallbacks, 1ull);
     R c = -k4 * (R)sc.vol0 * det3(Fg);
     const R pm = (R)sc.pmass;
-    int base[3];
-    R fx[3];
-    bin_particle(x, inv_dx, sc.shape, base, fx);
-    R rec[PAYLOAD];
     rec[0] = fx[0]; rec[1] = fx[1]; rec[2] = fx[2]; rec[3] = pm;
 #pragma unroll
     for (int i = 0; i < 3; ++i) rec[4 + i] = pm * v[i];
 #pragma unroll
     for (int i = 0; i < 9; ++i) rec[7 + i] = (pm * C[i] + dt * (c * tau[i])) * dx;
     if (!finite9(tau)) raise_status(ctx.status, MPM_ERR_NONFINITE);
-    store_record(payload, sidx, rec);
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256, 3)
+prepass_kernel(Ctx ctx, MpmParticles P, R* __restrict__ payload, int t) {
+    long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= ctx.n) return;
+    const MpmScene& sc = ctx.scenes[ctx.scene_of[p]];
+    R x[3], v[3], C[9], F[9], Fg[9];
+    ld3<R>(P.x, p, P.sp3, P.sc3, x);
+    ld3<R>(P.v, p, P.sp3, P.sc3, v);
+    ld9<R>(P.C, p, P.sp9, P.sc9, C);
+    ld9<R>(P.F, p, P.sp9, P.sc9, F);
+    load_Fg<R>(ctx, sc, P, p, t, Fg, nullptr);
+    int base[3];
+    R fx[3];
+    bin_particle(x, (R)(1.0 / sc.dx), sc.shape, base, fx);
+    R rec[PAYLOAD];
+    p2g_record<R>(ctx, sc, fx, v, C, F, Fg, rec);
+    store_record(payload, p, rec);
 }
 
 // ---------------------------------------------------------------------------
@@ -490,7 +498,8 @@ __device__ __forceinline__ void store_acc(R* __restrict__ S, long long cap, int 
 
 template <typename R, int MODE, int OXB>
 __global__ void __launch_bounds__(128)
-cell_sums_kernel(Ctx ctx, const R* __restrict__ payload, R* __restrict__ S, long long cap) {
+cell_sums_kernel(Ctx ctx, const unsigned* __restrict__ perm, const R* __restrict__ payload, R* __restrict__ S,
+                 long long cap) {
     const int nseg = *ctx.n_seg;
     for (int id = blockIdx.x * blockDim.x + threadIdx.x; id < nseg; id += gridDim.x * blockDim.x) {
         const int first = ctx.seg_first[id], last = ctx.seg_last[id];
@@ -500,7 +509,7 @@ cell_sums_kernel(Ctx ctx, const R* __restrict__ payload, R* __restrict__ S, long
             zero_acc<R, OXB>(acc);
             for (int q = first; q < last; ++q) {
                 R r[PAYLOAD];
-                load_record(payload, q, r);
+                load_record(payload, perm[q], r);
                 accumulate_record<R, MODE, OXB>(r, ox0, acc);
             }
             store_acc<R, OXB>(S, cap, id, ox0, acc);
@@ -730,9 +739,10 @@ __device__ __forceinline__ void unmark_cell(const Ctx& ctx, const SceneAux& ax, 
 // G2P + advection + F update (transfer.py:61-79); writes the output state in
 // the input's particle order and clears the cell marks of this step.
 // ---------------------------------------------------------------------------
-template <typename R>
-__global__ void __launch_bounds__(256, sizeof(R) == 4 ? 4 : 2)
-g2p_kernel(Ctx ctx, Tape<R> tp, MpmParticles in, MpmParticles out, int advect) {
+template <typename R, bool EMIT>
+__global__ void __launch_bounds__(256, EMIT ? (sizeof(R) == 4 ? 3 : 1) : (sizeof(R) == 4 ? 4 : 2))
+g2p_kernel(Ctx ctx, Tape<R> tp, MpmParticles in, MpmParticles out, int advect, unsigned* __restrict__ keys,
+           R* __restrict__ payload, int t) {
     long long sidx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (sidx >= ctx.n) return;
     long long p = tp.perm[sidx];
@@ -810,6 +820,15 @@ g2p_kernel(Ctx ctx, Tape<R> tp, MpmParticles in, MpmParticles out, int advect) {
     if (!finite9(Fn) || !(xn[0] * R(0) == R(0) && xn[1] * R(0) == R(0) && xn[2] * R(0) == R(0)))
         raise_status(ctx.status, MPM_ERR_NONFINITE);
     unmark_cell(ctx, ax, tp.skeys, sidx);
+    if constexpr (EMIT) {
+        // the next step's binning and P2G record of the new state (what the
+        // bin and prepass kernels of step t+1 would compute from memory)
+        R fxn[3], Fg[9], rec[PAYLOAD];
+        keys[p] = particle_key<R>(ctx, sc, ax, xn, fxn);
+        load_Fg<R>(ctx, sc, in, p, t + 1, Fg, nullptr);
+        p2g_record<R>(ctx, sc, fxn, nv, nC, Fn, Fg, rec);
+        store_record(payload, p, rec);
+    }
 }
 
 // ---------------------------------------------------------------------------

@@ -197,10 +197,14 @@ class Plan:
 
     # -- steps ---------------------------------------------------------------
     def step_fwd(self, pin: L.MpmParticles, pout: L.MpmParticles, advect: bool, t: int,
-                 tape: Optional["TapeBuf"] = None, stream=None):
-        L.check(self.lib.mpm_step_fwd(self.handle, C.byref(pin), C.byref(pout), int(bool(advect)), int(t),
-                                      C.c_void_p(tape.ptr if tape is not None else 0),
-                                      C.c_void_p(stream_ptr(stream))), "mpm_step_fwd")
+                 tape: Optional["TapeBuf"] = None, stream=None, chained: bool = False, emit: bool = False):
+        """One forward step.  chained/emit: consecutive steps of a trajectory
+        (mpm_step_fwd_chain): emit forms the next step's cell keys and P2G
+        records in this step's G2P, chained uses them."""
+        flags = (L.MPM_FWD_CHAINED if chained else 0) | (L.MPM_FWD_EMIT if emit else 0)
+        L.check(self.lib.mpm_step_fwd_chain(self.handle, C.byref(pin), C.byref(pout), int(bool(advect)), int(t),
+                                            C.c_void_p(tape.ptr if tape is not None else 0), flags,
+                                            C.c_void_p(stream_ptr(stream))), "mpm_step_fwd")
 
     def step_bwd(self, pin: L.MpmParticles, out_C_ptr: int, ob: L.MpmCotangents, ib: L.MpmCotangents,
                  growth_grad: Optional[torch.Tensor], advect: bool, t: int, tape: "TapeBuf", stream=None):

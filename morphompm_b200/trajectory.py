@@ -94,7 +94,8 @@ class Rollout:
             cur.copy_(slab0)
             for t in range(self.n_steps):
                 nxt = self.seg_states[t + 1]
-                p.step_fwd(self._pp(cur), self._pp(nxt), self.advect, t, self.tapes[t], stream)
+                p.step_fwd(self._pp(cur), self._pp(nxt), self.advect, t, self.tapes[t], stream,
+                           chained=t > 0, emit=t + 1 < self.n_steps)
                 cur = nxt
             self.final.copy_(cur)
             return self.final
@@ -106,7 +107,8 @@ class Rollout:
                 nxt = self.ckpt[(t + 1) // self.k]
             else:
                 nxt = self.scratch[t % 2] if cur is not self.scratch[t % 2] else self.scratch[(t + 1) % 2]
-            p.step_fwd(self._pp(cur), self._pp(nxt), self.advect, t, None, stream)
+            p.step_fwd(self._pp(cur), self._pp(nxt), self.advect, t, None, stream,
+                       chained=t > 0, emit=t + 1 < self.n_steps)
             cur = nxt
         return self.final
 
@@ -147,7 +149,8 @@ class Rollout:
                 st[0].copy_(self.ckpt[seg])
                 for t in range(t0, t1):
                     j = t - t0
-                    p.step_fwd(self._pp(st[j]), self._pp(st[j + 1]), self.advect, t, self.tapes[j], stream)
+                    p.step_fwd(self._pp(st[j]), self._pp(st[j + 1]), self.advect, t, self.tapes[j], stream,
+                               chained=t > t0, emit=t + 1 < t1)
             for t in range(t1 - 1, t0 - 1, -1):
                 j = t - t0
                 s_in = self.seg_states[j]

@@ -85,7 +85,9 @@ typedef struct MpmParticles {
 } MpmParticles;
 
 /* Cotangents of a particle state.  Same layout rules as MpmParticles; the Fg
- * cotangent is always double (it carries the growth-parameter gradient). */
+ * cotangent is always double (it carries the growth-parameter gradient) and is
+ * indexed with the strides of F: element c of particle p at Fg[p*sp9 + c*sc9]
+ * (in doubles), so it must have the layout of the F cotangent. */
 typedef struct MpmCotangents {
     void *x, *v, *C, *F;
     double *Fg;              /* may be NULL when every scene uses growth_mode 1 */

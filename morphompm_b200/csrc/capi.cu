@@ -46,7 +46,7 @@ struct MpmPlan {
     int TN = 0, active_cap = 0;
     bool any_growth = false;
     // workspace offsets
-    size_t o_scenes, o_aux, o_scene_of, o_tile_scene, o_status, o_cell_seg, o_seg_first, o_seg_last, o_blk, o_tblk;
+    size_t o_scenes, o_aux, o_scene_of, o_tile_scene, o_status, o_cell_seg, o_blk, o_tblk;
     size_t o_tile_flag, o_keys, o_kalt0, o_valt0, o_kalt1, o_valt1, o_hist, o_totals, o_payload, o_sums;
     size_t o_dense_f = 0, o_dense_b = 0;
     long long n_nodes = 0;
@@ -58,7 +58,7 @@ struct MpmPlan {
     MpmParticles chain_state{};
     size_t ws_bytes = 0;
     // tape offsets
-    size_t t_skeys, t_perm, t_active, t_nact, t_grid, tape_bytes = 0;
+    size_t t_skeys, t_perm, t_seg_first, t_seg_last, t_nseg, t_active, t_nact, t_grid, tape_bytes = 0;
     char* ws = nullptr;
     const void* phi = nullptr;
     int n_sm = 148;
@@ -84,9 +84,9 @@ Ctx make_ctx(MpmPlan* P) {
     c.status = at<int>(P, P->o_status);
     c.fallbacks = reinterpret_cast<unsigned long long*>(P->ws + P->o_status + 64);
     c.cell_seg = at<int>(P, P->o_cell_seg);
-    c.seg_first = at<int>(P, P->o_seg_first);
-    c.seg_last = at<int>(P, P->o_seg_last);
-    c.n_seg = reinterpret_cast<int*>(P->ws + P->o_status + 32);
+    c.seg_first = nullptr;    // in the step's tape (bind_segments)
+    c.seg_last = nullptr;
+    c.n_seg = nullptr;
     c.blk_count = at<unsigned>(P, P->o_blk);
     c.tile_flag = at<int>(P, P->o_tile_flag);
     c.phi = P->phi;
@@ -100,6 +100,13 @@ Ctx make_ctx(MpmPlan* P) {
     c.active_cap = P->active_cap;
     c.gap_thresh = P->tune.fp64_gap_thresh < 0 ? 0.0f : P->tune.fp64_gap_thresh;
     return c;
+}
+
+// the segment table of a step lives in its tape: the reverse step reuses it
+void bind_segments(MpmPlan* P, Ctx& c, const char* t) {
+    c.seg_first = reinterpret_cast<int*>(const_cast<char*>(t) + P->t_seg_first);
+    c.seg_last = reinterpret_cast<int*>(const_cast<char*>(t) + P->t_seg_last);
+    c.n_seg = reinterpret_cast<int*>(const_cast<char*>(t) + P->t_nseg);
 }
 
 template <typename R>
@@ -241,6 +248,7 @@ int step_fwd_R(MpmPlan* P, const MpmParticles& in, MpmParticles& out, int advect
                int flags, cudaStream_t st) {
     const bool chained = (flags & MPM_FWD_CHAINED) != 0, emit = (flags & MPM_FWD_EMIT) != 0;
     Ctx ctx = make_ctx(P);
+    bind_segments(P, ctx, tape);
     Tape<R> tp = make_tape<R>(P, tape);
     const int B = P->tune.particle_block;
     const int g = grid_for(P->n, B);
@@ -281,11 +289,18 @@ template <typename R>
 int step_bwd_R(MpmPlan* P, const MpmParticles& in, const void* outC, const MpmCotangents& ob, MpmCotangents& ib,
                double* growth_grad, int advect, int t, const char* tape, cudaStream_t st) {
     Ctx ctx = make_ctx(P);
+    bind_segments(P, ctx, tape);
     Tape<R> tp = make_tape<R>(P, const_cast<char*>(tape));
     const int B = P->tune.particle_block;
     const int g = grid_for(P->n, B);
     double* dbuf = at<double>(P, P->o_dbuf);
-    int rc = build_segments(P, ctx, tp.skeys, 0, st);
+    {
+        // the forward step's segment table is in the tape: restore the cell marks
+        Site s(P, MPM_K_MARK, 1, st);
+        const int blocks = (int)std::max<long long>(1, std::min<long long>((P->n + 255) / 256, (long long)P->n_sm * 8));
+        remark_cells_kernel<<<blocks, 256, 0, st>>>(ctx, tp.skeys);
+    }
+    int rc = check_launch();
     if (rc) return rc;
     {
         Site s(P, MPM_K_BWD_P2G, 2, st);
@@ -386,6 +401,9 @@ int mpm_plan_create(const MpmScene* scenes, int32_t n_scenes, int32_t real_bytes
     Layout tl;
     P->t_skeys = tl.take(n * 4);
     P->t_perm = tl.take(n * 4);
+    P->t_seg_first = tl.take(n * 4);
+    P->t_seg_last = tl.take(n * 4);
+    P->t_nseg = tl.take(4);
     P->t_active = tl.take((size_t)P->active_cap * 4);
     P->t_nact = tl.take(4);
     P->t_grid = tl.take((size_t)P->active_cap * P->TN * 4 * R);
@@ -399,8 +417,6 @@ int mpm_plan_create(const MpmScene* scenes, int32_t n_scenes, int32_t real_bytes
     P->o_status = L.take(128);
     P->nblk_seg = (int)((P->n + SEG_TILE - 1) / SEG_TILE);
     P->o_cell_seg = L.take((size_t)P->n_keys * 4);
-    P->o_seg_first = L.take(n * 4);
-    P->o_seg_last = L.take(n * 4);
     P->o_blk = L.take((size_t)P->nblk_seg * 4);
     P->nblk_tile = (int)((P->n_tiles + SEG_TILE - 1) / SEG_TILE);
     P->o_tblk = L.take((size_t)P->nblk_tile * 4);
@@ -736,6 +752,9 @@ bool noalloc_layout(MpmPlan& P, const MpmScene& sc, int real_bytes, SceneAux& a)
     Layout tl;
     P.t_skeys = tl.take(n * 4);
     P.t_perm = tl.take(n * 4);
+    P.t_seg_first = tl.take(n * 4);
+    P.t_seg_last = tl.take(n * 4);
+    P.t_nseg = tl.take(4);
     P.t_active = tl.take((size_t)P.active_cap * 4);
     P.t_nact = tl.take(4);
     P.t_grid = tl.take((size_t)P.active_cap * P.TN * 4 * R);
@@ -747,8 +766,6 @@ bool noalloc_layout(MpmPlan& P, const MpmScene& sc, int real_bytes, SceneAux& a)
     P.o_tile_scene = L.take(nt * 4);
     P.o_status = L.take(128);
     P.o_cell_seg = L.take((size_t)P.n_keys * 4);
-    P.o_seg_first = L.take(n * 4);
-    P.o_seg_last = L.take(n * 4);
     P.o_blk = L.take((size_t)P.nblk_seg * 4);
     P.nblk_tile = (int)((P.n_tiles + SEG_TILE - 1) / SEG_TILE);
     P.o_tblk = L.take((size_t)P.nblk_tile * 4);

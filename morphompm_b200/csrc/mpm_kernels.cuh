@@ -266,6 +266,15 @@ scan_counts_kernel(unsigned* __restrict__ cnt, int nblk, int* __restrict__ total
     }
 }
 
+// Reverse step: the segment table is the one the forward step recorded in the
+// tape; only the dense cell marks (cleared by the forward G2P) are restored.
+__global__ void __launch_bounds__(256)
+remark_cells_kernel(Ctx ctx, const unsigned* __restrict__ skeys) {
+    const int nseg = *ctx.n_seg;
+    for (int id = blockIdx.x * blockDim.x + threadIdx.x; id < nseg; id += gridDim.x * blockDim.x)
+        ctx.cell_seg[skeys[ctx.seg_first[id]]] = id + 1;
+}
+
 // Active-tile list: the tiles flagged by the segment count pass, in tile
 // order.  Per-block counts (warp-striped, coalesced), the block scan above,
 // then ranks from warp ballots; the flags are reset for the next step.

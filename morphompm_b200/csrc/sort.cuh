@@ -86,61 +86,75 @@ radix_rowscan_kernel(unsigned* __restrict__ hist, int nblk, const unsigned* __re
 }
 
 // Stable scatter.  vals_in == nullptr means the identity payload (slot index).
+// Warp w of a block owns the contiguous chunk [w*PER_WARP, (w+1)*PER_WARP) of
+// the block's tile, so the order (warp, round, lane) is the input order.
+// Pass 1 counts each warp's digits, one block-wide prefix turns the counts
+// into the warps' output offsets per digit, pass 2 scatters: a key's
+// position is its warp's running offset for its digit plus its rank among the
+// lanes of its round with the same digit (warp match masks).
 __global__ void __launch_bounds__(SORT_THREADS)
 radix_scatter_kernel(const unsigned* __restrict__ keys_in, const unsigned* __restrict__ vals_in, long long n,
                      int shift, const unsigned* __restrict__ offs, int nblk,
                      unsigned* __restrict__ keys_out, unsigned* __restrict__ vals_out) {
     constexpr int NW = SORT_THREADS / 32;
+    constexpr int PER_WARP = SORT_TILE / NW;   // SORT_ITEMS rounds of 32 keys
     __shared__ unsigned wcnt[NW][RADIX];
-    __shared__ unsigned base_d[RADIX];
-    __shared__ unsigned round_tot[RADIX];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int d = threadIdx.x; d < RADIX; d += SORT_THREADS) {
-        base_d[d] = offs[(long long)d * nblk + blockIdx.x];
+    const unsigned lt_mask = (1u << lane) - 1u;
+    for (int i = threadIdx.x; i < NW * RADIX; i += SORT_THREADS) (&wcnt[0][0])[i] = 0;
+    __syncthreads();
+    const long long wbase = (long long)blockIdx.x * SORT_TILE + (long long)warp * PER_WARP;
+    unsigned key[SORT_ITEMS], val[SORT_ITEMS];
+    // pass 1: digit counts of this warp's chunk
 #pragma unroll
-        for (int w = 0; w < NW; ++w) wcnt[w][d] = 0;
+    for (int r = 0; r < SORT_ITEMS; ++r) {
+        const long long q = wbase + (long long)r * 32 + lane;
+        const bool valid = q < n;
+        key[r] = valid ? keys_in[q] : 0u;
+        val[r] = valid ? (vals_in ? vals_in[q] : (unsigned)q) : 0u;
+        const unsigned dig = (key[r] >> shift) & (RADIX - 1);
+        const unsigned vmask = __ballot_sync(0xffffffffu, valid);
+        if (valid) {
+            const unsigned peers = __match_any_sync(vmask, dig);
+            if ((peers & lt_mask) == 0) wcnt[warp][dig] += __popc(peers);
+        }
+        __syncwarp();
     }
     __syncthreads();
-    long long base = (long long)blockIdx.x * SORT_TILE;
-    const unsigned lt_mask = (1u << lane) - 1u;
+    // per digit: exclusive prefix over the warps, from the block's offset
+    for (int d = threadIdx.x; d < RADIX; d += SORT_THREADS) {
+        unsigned run = offs[(long long)d * nblk + blockIdx.x];
+#pragma unroll
+        for (int w = 0; w < NW; ++w) {
+            const unsigned c = wcnt[w][d];
+            wcnt[w][d] = run;
+            run += c;
+        }
+    }
+    __syncthreads();
+    // pass 2: scatter
+#pragma unroll
     for (int r = 0; r < SORT_ITEMS; ++r) {
-        long long q = base + (long long)r * SORT_THREADS + threadIdx.x;
-        bool valid = q < n;
-        unsigned key = valid ? keys_in[q] : 0u;
-        unsigned val = valid ? (vals_in ? vals_in[q] : (unsigned)q) : 0u;
-        unsigned dig = (key >> shift) & (RADIX - 1);
-        unsigned vmask = __ballot_sync(0xffffffffu, valid);
-        unsigned peers = 0, rank = 0;
+        const long long q = wbase + (long long)r * 32 + lane;
+        const bool valid = q < n;
+        const unsigned dig = (key[r] >> shift) & (RADIX - 1);
+        const unsigned vmask = __ballot_sync(0xffffffffu, valid);
+        unsigned peers = 0, rank = 0, base = 0;
+        int leader = lane;
         if (valid) {
             peers = __match_any_sync(vmask, dig);
             rank = __popc(peers & lt_mask);
-            if (rank == 0) wcnt[warp][dig] = __popc(peers);
+            leader = __ffs(peers) - 1;
+            if (rank == 0) base = wcnt[warp][dig];
         }
-        __syncthreads();
-        // exclusive prefix over warps, per digit
-        for (int d = threadIdx.x; d < RADIX; d += SORT_THREADS) {
-            unsigned run = 0;
-#pragma unroll
-            for (int w = 0; w < NW; ++w) {
-                unsigned c = wcnt[w][d];
-                wcnt[w][d] = run;
-                run += c;
-            }
-            round_tot[d] = run;
-        }
-        __syncthreads();
+        base = __shfl_sync(0xffffffffu, base, leader);
         if (valid) {
-            unsigned pos = base_d[dig] + wcnt[warp][dig] + rank;
-            keys_out[pos] = key;
-            vals_out[pos] = val;
+            keys_out[base + rank] = key[r];
+            vals_out[base + rank] = val[r];
         }
-        __syncthreads();
-        for (int d = threadIdx.x; d < RADIX; d += SORT_THREADS) {
-            base_d[d] += round_tot[d];
-#pragma unroll
-            for (int w = 0; w < NW; ++w) wcnt[w][d] = 0;
-        }
-        __syncthreads();
+        __syncwarp();
+        if (valid && rank == 0) wcnt[warp][dig] = base + __popc(peers);
+        __syncwarp();
     }
 }
 

@@ -200,14 +200,24 @@ def kernel_bytes_per_particle(kind, w):
     fields it reads and writes, its payload record, 4-byte sort indices);
     node records are added separately."""
     table = {
-        "prepass": 24 * w + 16 * w + 4 + 4,        # x v C F (+ growth law) -> payload, perm, scene id
-        "p2g": 16 * w,                             # payload record once
-        "g2p": 12 * w + 24 * w + 4 + 4 + 4,        # x F -> x v C F, perm, key, scene id
-        "bwd_payload": 36 * w + 16 * w + 4 + 4,
-        "bwd_p2g": 16 * w,
+        "prepass": 24 * w + 16 * w + 4,            # x v C F (+ growth law) -> P2G record, scene id
+        "p2g": 16 * w + 4,                         # P2G record once, through perm
+        # chained step: x F -> x v C F, the next step's record and key; perm, old key, scene id
+        "g2p": 12 * w + 24 * w + 16 * w + 4 + 4 + 4 + 4,
+        "bwd_p2g": 36 * w + 4,                     # x F + the x v C F cotangents, through perm
         "bwd_particle": (24 + 9 + 24 + 24) * w + 8 + 4 + 4 + 4,
     }
     return table.get(kind)
+
+
+# DRAM bytes (read + write) per particle per launch of the heaviest kernels, from
+# one `ncu --set full` capture of a 2,092,825-particle batch of the config-4
+# generator (FP32, chained steps); their traffic grows in proportion to the
+# particles, so it is scaled to the workload.
+MEASURED_TRAFFIC_PER_PARTICLE = {
+    "bwd_particle": (526.156288e6 + 210.969088e6) / 2092825,
+    "g2p": (137.490688e6 + 339.093504e6) / 2092825,
+}
 
 
 def node_bytes(kind, w):
@@ -324,7 +334,10 @@ def main():
         achieved = alg / (avg_ms / 1e3) / 1e9
     roof = {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak, "peak_source": peak_src,
             "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
-            "traffic": None, "avg_launch_ms": avg_ms, "launches": nl}
+            "traffic": (MEASURED_TRAFFIC_PER_PARTICLE[dominant] * n_tot
+                        if dominant in MEASURED_TRAFFIC_PER_PARTICLE else None),
+            "traffic_source": "ncu dram bytes per launch, 2.09M-particle capture scaled by particles",
+            "avg_launch_ms": avg_ms, "launches": nl}
     # whole step against the algorithmic bytes per particle-step fwd+adj
     # (w*(156 + 32*G_touched/n), G_touched/n ~ 0.2 at 8 particles per cell)
     step_bytes = w * (156 + 32 * 0.2) * n_tot * a.mpm_steps

@@ -192,10 +192,10 @@ def load_tuned(scenes: List[dict], dtype) -> Optional[dict]:
 
 def autotune(scenes: List[dict], dtype=torch.float32, steps: int = 4, budget_s: float = 90.0,
              save: bool = False, verbose: bool = False) -> Dict:
-    """Time `steps` forward steps of the batch for every candidate schedule
-    (coordinate search: one knob at a time, starting from the defaults) and
-    return the fastest.  Results are deterministic whatever the schedule
-    (the summation order per node does not depend on it)."""
+    """Time a `steps`-step forward + adjoint trajectory of the batch for every
+    candidate schedule (coordinate search: one knob at a time, starting from
+    the defaults) and return the fastest.  Results are deterministic whatever
+    the schedule (the summation order per node does not depend on it)."""
     t_start = time.time()
     best = {"tile_xy": 4, "tile_z": 4, "scatter_ctas_per_sm": 1, "scatter_oxb": 3 if dtype == torch.float32 else 1,
             "particle_block": 256}
@@ -205,11 +205,11 @@ def autotune(scenes: List[dict], dtype=torch.float32, steps: int = 4, budget_s: 
         b = Batch(scenes, steps, dtype=dtype, tuning=cfg, ckpt_every=steps, active_cap=None)
         b.load(slab.to(b.plan.device), non_blocking=False)
         ro = b.rollout
-        ro.forward(b.slab0)
+        ro.run(b.slab0)
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
-        ro.forward(b.slab0)
+        ro.run(b.slab0)
         e1.record()
         torch.cuda.synchronize()
         return e0.elapsed_time(e1)

@@ -325,7 +325,7 @@ int step_bwd_R(MpmPlan* P, const MpmParticles& in, const void* outC, const MpmCo
     }
     if (want_dA) {
         Site s(P, MPM_K_REDUCE, 1, st);
-        scene_reduce_kernel<<<(int)P->scenes.size(), 256, 0, st>>>(ctx, dbuf, growth_grad, 1, 0);
+        scene_reduce_kernel<<<(int)P->scenes.size(), REDUCE_THREADS, 0, st>>>(ctx, dbuf, growth_grad, 1, 0);
     }
     return check_launch();
 }
@@ -656,7 +656,7 @@ int mpm_loss_detF(MpmPlan* P, const void* F, int64_t sp9, int64_t sc9, double* l
         loss_detF_kernel<float><<<g, 256, 0, st>>>(ctx, (const float*)F, sp9, sc9, dbuf, (float*)F_bar);
     else
         loss_detF_kernel<double><<<g, 256, 0, st>>>(ctx, (const double*)F, sp9, sc9, dbuf, (double*)F_bar);
-    scene_reduce_kernel<<<(int)P->scenes.size(), 256, 0, st>>>(ctx, dbuf, loss, 0, 0);
+    scene_reduce_kernel<<<(int)P->scenes.size(), REDUCE_THREADS, 0, st>>>(ctx, dbuf, loss, 0, 0);
     return check_launch();
 }
 
@@ -674,7 +674,7 @@ int mpm_loss_mse(MpmPlan* P, const void* x, int64_t sp3, int64_t sc3, const void
     else
         loss_mse_kernel<double><<<g, 256, 0, st>>>(ctx, (const double*)x, sp3, sc3, (const double*)x_obs, dbuf,
                                                    (double*)x_bar);
-    scene_reduce_kernel<<<(int)P->scenes.size(), 256, 0, st>>>(ctx, dbuf, loss, 0, 1);
+    scene_reduce_kernel<<<(int)P->scenes.size(), REDUCE_THREADS, 0, st>>>(ctx, dbuf, loss, 0, 1);
     return check_launch();
 }
 

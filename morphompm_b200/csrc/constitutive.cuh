@@ -435,11 +435,10 @@ __device__ __forceinline__ bool hencky_vjp_keep(const R* F, const R* Fg, R mu, R
 
 // ---------------------------------------------------------------------------
 // model dispatch.  Returns true when an FP32 Hencky evaluation went to FP64.
-// The stand-alone Hencky stress and VJP are called out of line so that their
-// register demand (the eigensolve, the FP64 recompute) does not inflate the
-// allocation of the kernels that fuse them; the reverse kernel's variants that
-// keep the eigendecomposition are inlined (out-of-line calls would pass their
-// arrays through the local-memory stack).
+// The eigensolves are inlined (an out-of-line call passes its arrays through
+// the local-memory stack); the stand-alone Hencky VJP and the rare FP64
+// recompute of the stress stay out of line so that their register demand does
+// not inflate the allocation of the kernels that fuse them.
 // ---------------------------------------------------------------------------
 template <typename R>
 __device__ __noinline__ bool hencky_stress_ool(const R* F, const R* Fg, R mu, R lam, float thresh, R* tau) {
@@ -453,7 +452,16 @@ __device__ __noinline__ bool hencky_vjp_ool(const R* F, const R* Fg, R mu, R lam
 template <typename R>
 __device__ __forceinline__ bool model_stress(const ModelParams<R>& P, float thresh, const R F[9], const R Fg[9],
                                              const R C[9], R tau[9]) {
-    if (P.kind == MPM_MODEL_HENCKY) return hencky_stress_ool<R>(F, Fg, P.mu, P.lam, thresh, tau);
+    if (P.kind == MPM_MODEL_HENCKY) {
+        // the eigensolve inline; only the rare FP32 -> FP64 recompute out of line
+        R Fgi[9], Fe[9], beta[3], V[9];
+        hencky_eig(F, Fg, Fgi, Fe, beta, V);
+        if constexpr (sizeof(R) == 4) {
+            if (sv_gap(beta) < thresh) return hencky_stress_ool<R>(F, Fg, P.mu, P.lam, thresh, tau);
+        }
+        hencky_tau_from_eig(beta, V, P.mu, P.lam, tau);
+        return false;
+    }
     if (P.kind == MPM_MODEL_HERSCHEL_BULKLEY) { hb_stress<R>(F, Fg, C, P, tau); return false; }
     nh_stress(F, Fg, P.mu, P.lam, tau);
     return false;

@@ -1062,23 +1062,34 @@ bwd_particle_kernel(Ctx ctx, Tape<R> tp, MpmParticles in, const R* __restrict__ 
 // out[s] = (accumulate ? out[s] : 0) + scale_s * sum_{slots of s} v
 // scale_s = 1 (mode 0) or 1/n_s (mode 1)
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256)
+constexpr int REDUCE_THREADS = 1024;
+__global__ void __launch_bounds__(REDUCE_THREADS)
 scene_reduce_kernel(Ctx ctx, const double* __restrict__ v, double* __restrict__ out, int accumulate, int mean) {
-    __shared__ double red[256];
-    const int s = blockIdx.x;
+    __shared__ double wsum[REDUCE_THREADS / 32];
+    const int s = blockIdx.x, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const MpmScene& sc = ctx.scenes[s];
-    double acc = 0.0;
-    for (long long i = sc.p_begin + threadIdx.x; i < sc.p_end; i += 256) acc += v[i];
-    red[threadIdx.x] = acc;
-    __syncthreads();
-    for (int w = 128; w > 0; w >>= 1) {
-        if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
-        __syncthreads();
+    // two interleaved chains per thread, then a fixed shuffle tree: the order
+    // depends only on the scene's size
+    double a0 = 0.0, a1 = 0.0;
+    long long i = sc.p_begin + threadIdx.x;
+    for (; i + REDUCE_THREADS < sc.p_end; i += 2 * REDUCE_THREADS) {
+        a0 += v[i];
+        a1 += v[i + REDUCE_THREADS];
     }
-    if (threadIdx.x == 0) {
-        double r = red[0];
-        if (mean) r /= (double)(sc.p_end - sc.p_begin > 0 ? sc.p_end - sc.p_begin : 1);
-        out[s] = accumulate ? out[s] + r : r;
+    if (i < sc.p_end) a0 += v[i];
+    double acc = a0 + a1;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+    if (lane == 0) wsum[warp] = acc;
+    __syncthreads();
+    if (warp == 0) {
+        double r = wsum[lane];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) r += __shfl_down_sync(0xffffffffu, r, o);
+        if (lane == 0) {
+            if (mean) r /= (double)(sc.p_end - sc.p_begin > 0 ? sc.p_end - sc.p_begin : 1);
+            out[s] = accumulate ? out[s] + r : r;
+        }
     }
 }
 

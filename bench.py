@@ -145,6 +145,37 @@ def cpu_baseline(scenes, seconds):
                       f"fwd+adj each, numpy FP64 oracle, 1 thread"}
 
 
+def cpp_reference_forward(seconds=4.0):
+    """The reference's own C++ FP32 forward solver (growth_solver.h, built into
+    oracle/_ref from the reference tree), one core, on the 4096-particle
+    free-swell cube of config 1 with Hencky stress (the solver's only model).
+    Forward only: the C++ code has no adjoint.  None when the library is absent."""
+    from oracle import growth_ref as G
+    if not G.available():
+        return None
+    from morphompm_b200 import scenes as S
+    c = S.config1()
+    n = c["x"].shape[0]
+    sp = c["dx"] / 2
+
+    def make():
+        r = G.RefSolver(c["shape"][0], c["dx"], c["E"], c["nu"], c["damping"])
+        r.add(c["x"], c["density"] * sp ** 3, c["density"])
+        r.set_growth(1.0 + c["growth_A"])
+        return r
+    r = make()
+    t0 = time.perf_counter()
+    r.step(c["dt"], 2)
+    per_step = (time.perf_counter() - t0) / 2
+    steps = max(2, int(seconds / max(per_step, 1e-6)))
+    r = make()
+    t0 = time.perf_counter()
+    r.step(c["dt"], steps)
+    dt = time.perf_counter() - t0
+    return {"value": n * steps / dt, "unit": "particle-steps/s (forward only)", "cores": 1, "kind": "reference",
+            "sample": f"config-1 cube, {n} particles, {steps} forward steps, Hencky, FP32, C++ (growth_solver.h)"}
+
+
 def run_reference(a):
     """--impl reference: the oracle port on all host cores (process pool over scenes)."""
     rank = int(os.environ.get("RANK", "0"))
@@ -364,6 +395,7 @@ def main():
         line["fp64_plain"] = plain_leg(scn, a, value, tuning)
     if rank == 0 and not a.no_cpu:
         line["cpu_baseline"] = cpu_baseline(scn, a.cpu_seconds)
+        line["cpu_reference_forward"] = cpp_reference_forward()
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -164,7 +164,8 @@ int mpm_step_fwd(MpmPlan* plan, const MpmParticles* in, MpmParticles* out, int32
  * pass also bins the new state and evaluates its stress (Fg of the growth law
  * at step_index + 1, or the same explicit Fg); a following call with
  * MPM_FWD_CHAINED then skips its binning and stress passes.  The results are
- * those of mpm_step_fwd.  A CHAINED call whose `in` (every pointer and stride)
+ * those of mpm_step_fwd.  The caller must not change the state or an explicit
+ * Fg between the EMIT call and the CHAINED call.  A CHAINED call whose `in` (every pointer and stride)
  * or step_index does not continue the last EMIT call, or that follows any
  * other forward call on the plan, returns MPM_ERR_ARG. */
 int mpm_step_fwd_chain(MpmPlan* plan, const MpmParticles* in, MpmParticles* out, int32_t advect,

@@ -183,6 +183,18 @@ int mpm_step_bwd(MpmPlan* plan, const MpmParticles* in, const void* out_C,
                  double* growth_grad, int32_t advect, int32_t step_index,
                  const void* tape, void* stream);
 
+/* mpm_step_bwd that also accumulates the material-parameter gradients: when
+ * material_grad is not NULL, material_grad[2 s] += d loss / d mu_s and
+ * material_grad[2 s + 1] += d loss / d lambda_s for every scene s (double,
+ * deterministic order; zero for Herschel-Bulkley scenes).  No counterpart in
+ * the reference, whose constitutive VJPs stop at F, Fg and C
+ * (constitutive.py:36-39, 62-75); d/dE and d/dnu follow on the host from
+ * mu = E / (2 (1 + nu)), lambda = E nu / ((1 + nu)(1 - 2 nu)). */
+int mpm_step_bwd_params(MpmPlan* plan, const MpmParticles* in, const void* out_C,
+                        const MpmCotangents* out_bar, MpmCotangents* in_bar,
+                        double* growth_grad, double* material_grad, int32_t advect,
+                        int32_t step_index, const void* tape, void* stream);
+
 /* Batched constitutive seam: tau = model.stress(F, Fg, C) for n particles of one
  * scene's model.  Replaces constitutive.py:88-89,126-132. Arrays (n,3,3) C-contiguous. */
 int mpm_stress(const MpmScene* scene, int32_t real_bytes, int64_t n, const void* F,

@@ -80,6 +80,8 @@ EXPORTS = {
     "mpm_step_fwd_chain": (i32, [vp, C.POINTER(MpmParticles), C.POINTER(MpmParticles), i32, i32, vp, i32, vp]),
     "mpm_step_bwd": (i32, [vp, C.POINTER(MpmParticles), vp, C.POINTER(MpmCotangents),
                            C.POINTER(MpmCotangents), vp, i32, i32, vp, vp]),
+    "mpm_step_bwd_params": (i32, [vp, C.POINTER(MpmParticles), vp, C.POINTER(MpmCotangents),
+                                  C.POINTER(MpmCotangents), vp, vp, i32, i32, vp, vp]),
     "mpm_stress": (i32, [C.POINTER(MpmScene), i32, i64, vp, vp, vp, vp, vp]),
     "mpm_stress_vjp": (i32, [C.POINTER(MpmScene), i32, i64, vp, vp, vp, vp, vp, vp, vp, vp]),
     "mpm_bin_keys": (i32, [C.POINTER(MpmScene), i32, i64, vp, vp, vp]),

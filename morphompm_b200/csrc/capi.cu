@@ -287,7 +287,7 @@ int step_fwd_R(MpmPlan* P, const MpmParticles& in, MpmParticles& out, int advect
 
 template <typename R>
 int step_bwd_R(MpmPlan* P, const MpmParticles& in, const void* outC, const MpmCotangents& ob, MpmCotangents& ib,
-               double* growth_grad, int advect, int t, const char* tape, cudaStream_t st) {
+               double* growth_grad, double* material_grad, int advect, int t, const char* tape, cudaStream_t st) {
     Ctx ctx = make_ctx(P);
     bind_segments(P, ctx, tape);
     Tape<R> tp = make_tape<R>(P, const_cast<char*>(tape));
@@ -318,14 +318,25 @@ int step_bwd_R(MpmPlan* P, const MpmParticles& in, const void* outC, const MpmCo
     }
     if (rc) return rc;
     bool want_dA = growth_grad != nullptr && P->any_growth;
+    double* dmat = dbuf + P->n;     // material gradients per slot: mu, then lambda
     {
         Site s(P, MPM_K_BWD_PARTICLE, 1, st);
-        bwd_particle_kernel<R><<<g, B, 0, st>>>(ctx, tp, in, static_cast<const R*>(outC), ob, ib,
-                                                   want_dA ? dbuf : nullptr, advect, t);
+        if (material_grad)
+            bwd_particle_kernel<R, true><<<g, B, 0, st>>>(ctx, tp, in, static_cast<const R*>(outC), ob, ib,
+                                                          want_dA ? dbuf : nullptr, dmat, advect, t);
+        else
+            bwd_particle_kernel<R, false><<<g, B, 0, st>>>(ctx, tp, in, static_cast<const R*>(outC), ob, ib,
+                                                           want_dA ? dbuf : nullptr, nullptr, advect, t);
     }
     if (want_dA) {
         Site s(P, MPM_K_REDUCE, 1, st);
         scene_reduce_kernel<<<(int)P->scenes.size(), REDUCE_THREADS, 0, st>>>(ctx, dbuf, growth_grad, 1, 0);
+    }
+    if (material_grad) {
+        Site s(P, MPM_K_REDUCE, 2, st);
+        scene_reduce_kernel<<<(int)P->scenes.size(), REDUCE_THREADS, 0, st>>>(ctx, dmat, material_grad, 1, 0, 2);
+        scene_reduce_kernel<<<(int)P->scenes.size(), REDUCE_THREADS, 0, st>>>(ctx, dmat + P->n, material_grad + 1,
+                                                                             1, 0, 2);
     }
     return check_launch();
 }
@@ -432,7 +443,7 @@ int mpm_plan_create(const MpmScene* scenes, int32_t n_scenes, int32_t real_bytes
     P->o_sums = L.take(27 * n * 4 * R);
     P->o_dense_f = L.take((size_t)P->n_nodes * 4 * R);
     P->o_dense_b = L.take((size_t)P->n_nodes * 4 * R);
-    P->o_dbuf = L.take(n * 8);
+    P->o_dbuf = L.take(3 * n * 8);      // dL/dA, dL/dmu, dL/dlambda per slot
     P->o_tape = L.take(P->tape_bytes);
     P->ws_bytes = L.off;
     *out = P;
@@ -580,9 +591,9 @@ int mpm_step_fwd(MpmPlan* P, const MpmParticles* in, MpmParticles* out, int32_t 
     return mpm_step_fwd_chain(P, in, out, advect, step_index, tape, 0, stream);
 }
 
-int mpm_step_bwd(MpmPlan* P, const MpmParticles* in, const void* out_C, const MpmCotangents* out_bar,
-                 MpmCotangents* in_bar, double* growth_grad, int32_t advect, int32_t step_index, const void* tape,
-                 void* stream) {
+int mpm_step_bwd_params(MpmPlan* P, const MpmParticles* in, const void* out_C, const MpmCotangents* out_bar,
+                        MpmCotangents* in_bar, double* growth_grad, double* material_grad, int32_t advect,
+                        int32_t step_index, const void* tape, void* stream) {
     if (!P || !P->ws || !in || !out_C || !out_bar || !in_bar || !tape) return MPM_ERR_ARG;
     if (!out_bar->x || !out_bar->v || !out_bar->C || !out_bar->F || !in_bar->x || !in_bar->v || !in_bar->C ||
         !in_bar->F)
@@ -594,10 +605,17 @@ int mpm_step_bwd(MpmPlan* P, const MpmParticles* in, const void* out_C, const Mp
     if (reinterpret_cast<uintptr_t>(tape) % ALIGN) return MPM_ERR_ARG;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     return P->real_bytes == 4
-               ? step_bwd_R<float>(P, *in, out_C, *out_bar, *in_bar, growth_grad, advect, step_index,
+               ? step_bwd_R<float>(P, *in, out_C, *out_bar, *in_bar, growth_grad, material_grad, advect, step_index,
                                    static_cast<const char*>(tape), st)
-               : step_bwd_R<double>(P, *in, out_C, *out_bar, *in_bar, growth_grad, advect, step_index,
-                                    static_cast<const char*>(tape), st);
+               : step_bwd_R<double>(P, *in, out_C, *out_bar, *in_bar, growth_grad, material_grad, advect,
+                                    step_index, static_cast<const char*>(tape), st);
+}
+
+int mpm_step_bwd(MpmPlan* P, const MpmParticles* in, const void* out_C, const MpmCotangents* out_bar,
+                 MpmCotangents* in_bar, double* growth_grad, int32_t advect, int32_t step_index, const void* tape,
+                 void* stream) {
+    return mpm_step_bwd_params(P, in, out_C, out_bar, in_bar, growth_grad, nullptr, advect, step_index, tape,
+                               stream);
 }
 
 int mpm_stress(const MpmScene* scene, int32_t real_bytes, int64_t n, const void* F, const void* Fg, const void* C,

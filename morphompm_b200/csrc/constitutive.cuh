@@ -496,4 +496,47 @@ __device__ __forceinline__ bool model_vjp_keep(const ModelParams<R>& P, float th
     return model_vjp(P, thresh, F, Fg, C, tb, Fb, Fgb, Cb);
 }
 
+// ---------------------------------------------------------------------------
+// Material-parameter gradients of one particle (no counterpart in the
+// reference): g[0] = <tau_bar, d tau / d mu>, g[1] = <tau_bar, d tau / d lambda>.
+//   neo-Hookean: d tau/d mu = Fe Fe^T - I,      d tau/d lambda = ln J I
+//   Hencky:      d tau/d mu = V diag(ln beta) V^T, d tau/d lambda = 1/2 sum ln beta I
+// (Hencky from the eigendecomposition kept for the VJP, keep = {beta, V, flag}).
+// Herschel-Bulkley has no Lame parameters: zero.
+// ---------------------------------------------------------------------------
+template <typename R>
+__device__ __forceinline__ void model_param_grad(const ModelParams<R>& P, const R F[9], const R Fg[9],
+                                                 const R keep[13], const R tb[9], double g[2]) {
+    g[0] = 0.0;
+    g[1] = 0.0;
+    const R tr = tb[0] + tb[4] + tb[8];
+    if (P.kind == MPM_MODEL_NEOHOOKEAN) {
+        R Fgi[9], Fe[9], b[9];
+        inv3(Fg, Fgi);
+        mm(F, Fgi, Fe);
+        mmT(Fe, Fe, b);
+        R s = 0;
+#pragma unroll
+        for (int i = 0; i < 9; ++i) s += tb[i] * (b[i] - ((i % 4 == 0) ? R(1) : R(0)));
+        g[0] = (double)s;
+        g[1] = (double)(d_log(det3(Fe)) * tr);
+    } else if (P.kind == MPM_MODEL_HENCKY) {
+        const R lb[3] = {d_log(keep[0]), d_log(keep[1]), d_log(keep[2])};
+        const R* V = keep + 3;
+        R s = 0;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            // (V^T tb V)_kk = sum_ij V_ik tb_ij V_jk
+            R q = 0;
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+#pragma unroll
+                for (int j = 0; j < 3; ++j) q += V[3 * i + k] * tb[3 * i + j] * V[3 * j + k];
+            s += lb[k] * q;
+        }
+        g[0] = (double)s;
+        g[1] = (double)(R(0.5) * (lb[0] + lb[1] + lb[2]) * tr);
+    }
+}
+
 }  // namespace mpm

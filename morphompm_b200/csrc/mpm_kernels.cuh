@@ -847,10 +847,13 @@ g2p_kernel(Ctx ctx, Tape<R> tp, MpmParticles in, MpmParticles out, int advect, u
 // with M1 = k4 Cn_b'^T, M2 = pm C^T + dt sk^T, and the weight-only terms are
 // summed once per particle: x_b -= M1 sum(w gv) + M2 sum(w mb).
 // ---------------------------------------------------------------------------
-template <typename R>
+// MAT: also the material-parameter gradients per slot, dmat[sidx] (mu) and
+// dmat[n + sidx] (lambda).
+template <typename R, bool MAT>
 __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 2 : 1)
 bwd_particle_kernel(Ctx ctx, Tape<R> tp, MpmParticles in, const R* __restrict__ outC,
-                    MpmCotangents ob, MpmCotangents ib, double* __restrict__ dA, int advect, int t) {
+                    MpmCotangents ob, MpmCotangents ib, double* __restrict__ dA, double* __restrict__ dmat,
+                    int advect, int t) {
     long long sidx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (sidx >= ctx.n) return;
     long long p = tp.perm[sidx];
@@ -1027,6 +1030,12 @@ bwd_particle_kernel(Ctx ctx, Tape<R> tp, MpmParticles in, const R* __restrict__ 
     }
     fb |= model_vjp_keep(M, ctx.gap_thresh, F, Fg, C, taub, keep, Fb2, Fgb, Cb2);
     if (fb) atomicAdd(ctx.fallbacks, 1ull);
+    if constexpr (MAT) {
+        double gm[2];
+        model_param_grad(M, F, Fg, keep, taub, gm);
+        dmat[sidx] = gm[0];
+        dmat[ctx.n + sidx] = gm[1];
+    }
 #pragma unroll
     for (int i = 0; i < 9; ++i) {
         Fb[i] += Fb2[i];
@@ -1059,12 +1068,13 @@ bwd_particle_kernel(Ctx ctx, Tape<R> tp, MpmParticles in, const R* __restrict__ 
 
 // ---------------------------------------------------------------------------
 // deterministic per-scene reduction of a per-slot double buffer:
-// out[s] = (accumulate ? out[s] : 0) + scale_s * sum_{slots of s} v
+// out[s * stride] = (accumulate ? out[s * stride] : 0) + scale_s * sum_{slots of s} v
 // scale_s = 1 (mode 0) or 1/n_s (mode 1)
 // ---------------------------------------------------------------------------
 constexpr int REDUCE_THREADS = 1024;
 __global__ void __launch_bounds__(REDUCE_THREADS)
-scene_reduce_kernel(Ctx ctx, const double* __restrict__ v, double* __restrict__ out, int accumulate, int mean) {
+scene_reduce_kernel(Ctx ctx, const double* __restrict__ v, double* __restrict__ out, int accumulate, int mean,
+                    int stride = 1) {
     __shared__ double wsum[REDUCE_THREADS / 32];
     const int s = blockIdx.x, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const MpmScene& sc = ctx.scenes[s];
@@ -1088,7 +1098,7 @@ scene_reduce_kernel(Ctx ctx, const double* __restrict__ v, double* __restrict__ 
         for (int o = 16; o > 0; o >>= 1) r += __shfl_down_sync(0xffffffffu, r, o);
         if (lane == 0) {
             if (mean) r /= (double)(sc.p_end - sc.p_begin > 0 ? sc.p_end - sc.p_begin : 1);
-            out[s] = accumulate ? out[s] + r : r;
+            out[(long long)s * stride] = accumulate ? out[(long long)s * stride] + r : r;
         }
     }
 }

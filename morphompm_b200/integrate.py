@@ -110,3 +110,42 @@ def dloss_dg(pts, model, cfg, g, n_steps, advect, loss: str = "detF", x_obs=None
     L = float(ro.loss.sum().item())
     dg = float(ro.Fg_bar[0].sum().item() + ro.Fg_bar[4].sum().item() + ro.Fg_bar[8].sum().item())
     return L, dg
+
+
+def lame_to_young(mu_bar: float, lam_bar: float, E: float, nu: float):
+    """d/dE and d/dnu from d/dmu and d/dlambda: mu = E/(2(1+nu)),
+    lambda = E nu/((1+nu)(1-2nu))."""
+    dmu_dE = 1.0 / (2.0 * (1.0 + nu))
+    dmu_dnu = -E / (2.0 * (1.0 + nu) ** 2)
+    dlam_dE = nu / ((1.0 + nu) * (1.0 - 2.0 * nu))
+    dlam_dnu = E * (1.0 + 2.0 * nu * nu) / ((1.0 + nu) ** 2 * (1.0 - 2.0 * nu) ** 2)
+    return mu_bar * dmu_dE + lam_bar * dlam_dE, mu_bar * dmu_dnu + lam_bar * dlam_dnu
+
+
+def dloss_dparams(pts, model, cfg, g, n_steps, advect, loss: str = "detF", x_obs=None,
+                  ckpt_every: Optional[int] = None):
+    """Loss of the final state and its gradient with respect to the growth
+    factor g (Fg = g I) and the material parameters: returns
+    (L, {"g", "mu", "lam", "E", "nu"}).  The material-parameter gradients have
+    no counterpart in the reference (its VJPs stop at F, Fg and C); they come
+    from mpm_step_bwd_params.  Elastic models only (mu, lambda of the model)."""
+    from .trajectory import Rollout
+    p = to_device(pts).contiguous()
+    n = p.shape[0]
+    plan = get_plan([scene_spec(cfg, model, n)], p.dtype, p.device)
+    Fg = torch.zeros(9, n, dtype=p.dtype, device=p.device)
+    for i in range(3):
+        Fg[4 * i] = g
+    xo = None
+    if loss == "mse":
+        xo = to_device(x_obs, p.dtype, p.device).reshape(n, 3).t().contiguous()
+    ro = Rollout(plan, n_steps, advect=advect, ckpt_every=ckpt_every, Fg=Fg, loss=loss, x_obs=xo,
+                 material_grads=True)
+    ro.run(_slab_from_points(p))
+    L = float(ro.loss.sum().item())
+    dg = float(ro.Fg_bar[0].sum().item() + ro.Fg_bar[4].sum().item() + ro.Fg_bar[8].sum().item())
+    mu_b, lam_b = (float(v) for v in ro.material_grad[0].tolist())
+    mu, lam = float(model.mu), float(model.lam)
+    E, nu = mu * (3.0 * lam + 2.0 * mu) / (lam + mu), lam / (2.0 * (lam + mu))
+    dE, dnu = lame_to_young(mu_b, lam_b, E, nu)
+    return L, {"g": dg, "mu": mu_b, "lam": lam_b, "E": dE, "nu": dnu}

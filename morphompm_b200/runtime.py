@@ -207,11 +207,22 @@ class Plan:
                                             C.c_void_p(stream_ptr(stream))), "mpm_step_fwd")
 
     def step_bwd(self, pin: L.MpmParticles, out_C_ptr: int, ob: L.MpmCotangents, ib: L.MpmCotangents,
-                 growth_grad: Optional[torch.Tensor], advect: bool, t: int, tape: "TapeBuf", stream=None):
+                 growth_grad: Optional[torch.Tensor], advect: bool, t: int, tape: "TapeBuf", stream=None,
+                 material_grad: Optional[torch.Tensor] = None):
+        """Reverse of one step.  growth_grad (S,) and material_grad (S, 2:
+        d/dmu, d/dlambda) are float64 accumulators, or None."""
         gg = growth_grad.data_ptr() if growth_grad is not None else 0
-        L.check(self.lib.mpm_step_bwd(self.handle, C.byref(pin), C.c_void_p(out_C_ptr), C.byref(ob), C.byref(ib),
-                                      C.c_void_p(gg), int(bool(advect)), int(t), C.c_void_p(tape.ptr),
-                                      C.c_void_p(stream_ptr(stream))), "mpm_step_bwd")
+        if material_grad is None:
+            L.check(self.lib.mpm_step_bwd(self.handle, C.byref(pin), C.c_void_p(out_C_ptr), C.byref(ob),
+                                          C.byref(ib), C.c_void_p(gg), int(bool(advect)), int(t),
+                                          C.c_void_p(tape.ptr), C.c_void_p(stream_ptr(stream))), "mpm_step_bwd")
+            return
+        assert material_grad.dtype == torch.float64 and material_grad.is_contiguous()
+        assert material_grad.numel() == 2 * len(self.scenes)
+        L.check(self.lib.mpm_step_bwd_params(self.handle, C.byref(pin), C.c_void_p(out_C_ptr), C.byref(ob),
+                                             C.byref(ib), C.c_void_p(gg), C.c_void_p(material_grad.data_ptr()),
+                                             int(bool(advect)), int(t), C.c_void_p(tape.ptr),
+                                             C.c_void_p(stream_ptr(stream))), "mpm_step_bwd_params")
 
     def loss_detF(self, F_ptr: int, sp9: int, sc9: int, loss: torch.Tensor, F_bar_ptr: int = 0, stream=None):
         L.check(self.lib.mpm_loss_detF(self.handle, C.c_void_p(F_ptr), sp9, sc9, C.c_void_p(loss.data_ptr()),

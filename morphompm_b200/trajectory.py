@@ -46,7 +46,8 @@ class Rollout:
     """
 
     def __init__(self, plan: Plan, n_steps: int, advect: bool = True, ckpt_every: Optional[int] = None,
-                 Fg: Optional[torch.Tensor] = None, loss: str = "detF", x_obs: Optional[torch.Tensor] = None):
+                 Fg: Optional[torch.Tensor] = None, loss: str = "detF", x_obs: Optional[torch.Tensor] = None,
+                 material_grads: bool = False):
         self.plan = plan
         self.n_steps = int(n_steps)
         self.advect = bool(advect)
@@ -70,6 +71,8 @@ class Rollout:
         S = len(plan.scenes)
         self.loss = torch.zeros(S, dtype=torch.float64, device=dev)
         self.growth_grad = torch.zeros(S, dtype=torch.float64, device=dev)
+        # d loss / d (mu, lambda) per scene, when asked for
+        self.material_grad = torch.zeros(S, 2, dtype=torch.float64, device=dev) if material_grads else None
         self.bar0 = None
         self.graph = None
 
@@ -140,6 +143,8 @@ class Rollout:
         if bar_T is not None and bar_T is not self.bars[0]:
             self.bars[0].copy_(bar_T)
         self.growth_grad.zero_()
+        if self.material_grad is not None:
+            self.material_grad.zero_()
         cur_bar, nxt_bar = self.bars[0], self.bars[1]
         for seg in range(self.n_seg - 1, -1, -1):
             t0 = seg * self.k
@@ -159,7 +164,8 @@ class Rollout:
                 es = s_out.element_size()
                 p.step_bwd(self._pp(s_in), s_out.data_ptr() + 6 * n * es,
                            slab_cotangents(cur_bar, self.Fg_bar), slab_cotangents(nxt_bar, self.Fg_bar),
-                           self.growth_grad, self.advect, t, self.tapes[j], stream)
+                           self.growth_grad, self.advect, t, self.tapes[j], stream,
+                           material_grad=self.material_grad)
                 cur_bar, nxt_bar = nxt_bar, cur_bar
         self.bar0 = cur_bar
         return cur_bar

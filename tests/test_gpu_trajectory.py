@@ -148,3 +148,32 @@ def test_config1_free_swell_fp64_matches_oracle_1e10():
     assert res[torch.float64][0] <= 1e-10, res
     assert res[torch.float32][0] <= 1e-4, res
     assert abs(np.mean(np.linalg.det(st.F)) - 1.1 ** 3) < 0.1
+
+
+@pytest.mark.parametrize("kind", ["nh", "hencky"])
+def test_material_gradients_vs_fd_fp64(kind):
+    """d loss / d (E, nu) of a device FP64 trajectory (mpm_step_bwd_params)
+    against central differences of the loss in E and nu."""
+    from morphompm_b200 import integrate
+    from morphompm_b200.config import Material
+    from morphompm_b200.constitutive import NeoHookean, Hencky
+    rng = np.random.default_rng(5)
+    pts = rng.uniform(0.3, 0.6, size=(60, 3))
+    cfg = _cfg(N=12, dx=1 / 12, dt=4e-4, sp=1 / 24, wall=2)
+    x_obs = pts + 0.02 * rng.standard_normal(pts.shape)
+    cls = {"nh": NeoHookean, "hencky": Hencky}[kind]
+    E, nu = 2.0e4, 0.28
+    for loss in ("detF", "mse"):
+        L, grads = integrate.dloss_dparams(pts, cls(Material(E=E, nu=nu)), cfg, 1.2, 5, True, loss=loss,
+                                           x_obs=x_obs)
+        L0, dg = integrate.dloss_dg(pts, cls(Material(E=E, nu=nu)), cfg, 1.2, 5, True, loss=loss, x_obs=x_obs)
+        assert L == L0 and grads["g"] == dg
+        for name, h in (("E", 1e-4 * E), ("nu", 1e-5)):
+            kp = dict(E=E, nu=nu)
+            km = dict(E=E, nu=nu)
+            kp[name] += h
+            km[name] -= h
+            fp, _ = integrate.dloss_dg(pts, cls(Material(**kp)), cfg, 1.2, 5, True, loss=loss, x_obs=x_obs)
+            fm, _ = integrate.dloss_dg(pts, cls(Material(**km)), cfg, 1.2, 5, True, loss=loss, x_obs=x_obs)
+            fd = (fp - fm) / (2 * h)
+            assert abs(grads[name] - fd) < 1e-6 * max(abs(fd), 1e-12) + 1e-14, (kind, loss, name, grads[name], fd)

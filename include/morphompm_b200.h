@@ -141,6 +141,16 @@ int mpm_plan_active_tiles(MpmPlan* plan, const void* tape, int32_t* n_active, vo
  * graph's launches are counted once, at capture). */
 int64_t mpm_plan_launch_count(const MpmPlan* plan);
 
+/* Replace the physical parameters of the plan's scenes (growth amplitude and
+ * ramp, Lame and Herschel-Bulkley parameters, damping, dt, dx, masses,
+ * gravity, walls ...) without rebuilding it.  The structure must not change:
+ * the same number of scenes with the same p_begin/p_end, shape, model and
+ * growth_mode, else MPM_ERR_ARG.  Kernels read the table from device memory,
+ * so a captured CUDA graph replays with the new values.  Ends any chain of
+ * mpm_step_fwd_chain calls.  Synchronises `stream`.  No counterpart in the
+ * reference (its scene parameters are Python objects rebuilt per call). */
+int mpm_plan_update_scenes(MpmPlan* plan, const MpmScene* scenes, int32_t n_scenes, void* stream);
+
 /* Optional per-particle growth field phi_p (growth_mode 1), real type. */
 int mpm_plan_set_growth_field(MpmPlan* plan, const void* phi);
 

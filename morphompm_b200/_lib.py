@@ -76,6 +76,7 @@ EXPORTS = {
     "mpm_plan_profile_end": (i32, [vp, C.POINTER(f64), C.POINTER(i32)]),
     "mpm_plan_launch_count": (i64, [vp]),
     "mpm_plan_active_tiles": (i32, [vp, vp, C.POINTER(i32), vp]),
+    "mpm_plan_update_scenes": (i32, [vp, C.POINTER(MpmScene), i32, vp]),
     "mpm_step_fwd": (i32, [vp, C.POINTER(MpmParticles), C.POINTER(MpmParticles), i32, i32, vp, vp]),
     "mpm_step_fwd_chain": (i32, [vp, C.POINTER(MpmParticles), C.POINTER(MpmParticles), i32, i32, vp, i32, vp]),
     "mpm_step_bwd": (i32, [vp, C.POINTER(MpmParticles), vp, C.POINTER(MpmCotangents),

@@ -68,12 +68,15 @@ class Batch:
     def __init__(self, scenes: List[dict], n_steps: int, dtype=torch.float32, advect: bool = True,
                  ckpt_every=None, tuning: Optional[dict] = None, loss: str = "detF",
                  x_obs: Optional[np.ndarray] = None, device=None, active_cap="auto",
-                 memory_fraction: float = 0.75, slab_host: Optional[np.ndarray] = None):
+                 memory_fraction: float = 0.75, slab_host: Optional[np.ndarray] = None,
+                 material_grads: bool = False):
         """ckpt_every: int, None (store every step), "sqrt", or "auto" (largest
         interval that fits memory_fraction of the free device memory).
         active_cap: "auto" sizes the tapes' active-tile lists from a probe
-        forward run of slab_host (1.25x its maximum), None keeps every tile."""
-        self.scenes = scenes
+        forward run of slab_host (1.25x its maximum), None keeps every tile.
+        material_grads: also accumulate d loss / d (mu, lambda) per scene
+        (dloss_dmaterial, dloss_dE, dloss_dnu)."""
+        self.scenes = [dict(s) for s in scenes]   # set_params edits these copies
         self.n_steps = n_steps
         self.dtype = dtype
         self.specs = [scene_spec_from_dict(s) for s in scenes]
@@ -102,7 +105,7 @@ class Batch:
         if loss == "mse":
             xo = torch.as_tensor(np.ascontiguousarray(x_obs.T.astype(npd))).to(self.plan.device)
         self.rollout = Rollout(self.plan, n_steps, advect=advect, ckpt_every=self.ckpt_every, Fg=None, loss=loss,
-                               x_obs=xo)
+                               x_obs=xo, material_grads=material_grads)
         self.slab0 = torch.empty(SLAB_ROWS, self.n, dtype=dtype, device=self.plan.device)
         self.graph = None
 
@@ -157,6 +160,37 @@ class Batch:
     def dloss_dg(self) -> torch.Tensor:
         """d loss_s / d g_s (growth law g_s = 1 + A_s, so d/dA = d/dg)."""
         return self.rollout.growth_grad
+
+    @property
+    def dloss_dmaterial(self) -> torch.Tensor:
+        """(S, 2): d loss_s / d mu_s, d loss_s / d lambda_s (material_grads=True)."""
+        return self.rollout.material_grad
+
+    def dloss_dE_nu(self) -> np.ndarray:
+        """(S, 2) on the host: d loss_s / d E_s, d loss_s / d nu_s."""
+        from .integrate import lame_to_young
+        mg = self.rollout.material_grad.cpu().numpy()
+        out = np.zeros_like(mg)
+        for s, sc in enumerate(self.scenes):
+            out[s] = lame_to_young(mg[s, 0], mg[s, 1], float(sc["E"]), float(sc["nu"]))
+        return out
+
+    def set_params(self, growth_A=None, E=None, nu=None):
+        """New per-scene growth amplitudes and/or Young's moduli and Poisson
+        ratios (arrays of length S) for the same batch; the captured graph
+        replays with them (mpm_plan_update_scenes)."""
+        for s, sc in enumerate(self.scenes):
+            if growth_A is not None:
+                sc["growth_A"] = float(growth_A[s])
+            if E is not None:
+                sc["E"] = float(E[s])
+            if nu is not None:
+                sc["nu"] = float(nu[s])
+            if E is not None or nu is not None:
+                sc["mu"] = sc["E"] / (2.0 * (1.0 + sc["nu"]))
+                sc["lam"] = sc["E"] * sc["nu"] / ((1.0 + sc["nu"]) * (1.0 - 2.0 * sc["nu"]))
+        self.specs = [scene_spec_from_dict(s) for s in self.scenes]
+        self.plan.update_scenes(self.specs)
 
 
 # ---------------------------------------------------------------------------

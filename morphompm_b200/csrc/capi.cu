@@ -553,6 +553,26 @@ int mpm_plan_read_fp64_fallbacks(MpmPlan* P, int64_t* count, void* stream) {
     return cudaStreamSynchronize(st) == cudaSuccess ? MPM_OK : MPM_ERR_CUDA;
 }
 
+int mpm_plan_update_scenes(MpmPlan* P, const MpmScene* scenes, int32_t n_scenes, void* stream) {
+    if (!P || !P->ws || !scenes || n_scenes != (int)P->scenes.size()) return MPM_ERR_ARG;
+    for (int s = 0; s < n_scenes; ++s) {
+        const MpmScene& a = P->scenes[s];
+        const MpmScene& b = scenes[s];
+        if (!scene_ok(b) || a.p_begin != b.p_begin || a.p_end != b.p_end || a.model != b.model ||
+            a.growth_mode != b.growth_mode || a.shape[0] != b.shape[0] || a.shape[1] != b.shape[1] ||
+            a.shape[2] != b.shape[2])
+            return MPM_ERR_ARG;
+    }
+    for (int s = 0; s < n_scenes; ++s) P->scenes[s] = scenes[s];
+    P->chain_valid = false;     // records formed with the old parameters
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (cudaMemcpyAsync(P->ws + P->o_scenes, P->scenes.data(), sizeof(MpmScene) * P->scenes.size(),
+                        cudaMemcpyHostToDevice, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
+        return MPM_ERR_CUDA;
+    return MPM_OK;
+}
+
 int mpm_plan_set_growth_field(MpmPlan* P, const void* phi) {
     if (!P) return MPM_ERR_ARG;
     P->phi = phi;

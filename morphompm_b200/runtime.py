@@ -151,6 +151,18 @@ class Plan:
     def new_tape(self) -> "TapeBuf":
         return TapeBuf(self)
 
+    def update_scenes(self, scenes: List[SceneSpec], stream=None):
+        """New physical parameters for the same scene structure
+        (mpm_plan_update_scenes); captured graphs replay with them."""
+        scenes = list(scenes)
+        arr = (L.MpmScene * len(scenes))()
+        for i, sc in enumerate(scenes):
+            arr[i] = sc.to_c(self.offsets[i])
+        L.check(self.lib.mpm_plan_update_scenes(self.handle, arr, len(scenes), C.c_void_p(stream_ptr(stream))),
+                "mpm_plan_update_scenes")
+        self.scenes = scenes
+        self._c_scenes = arr
+
     def set_growth_field(self, phi: Optional[torch.Tensor]):
         if phi is not None:
             phi = phi.to(device=self.device, dtype=self.dtype).contiguous()

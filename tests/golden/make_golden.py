@@ -185,17 +185,46 @@ def make_c1_head(ref):
                         x=st.x, F=st.F, v=st.v)
 
 
+def make_io(ref_root):
+    """Files written by the reference's own I/O adapters (io.py:29-111) for a
+    small state and config, so that the device-side writers are checked byte
+    for byte."""
+    sys.path.insert(0, os.path.join(ref_root, "python"))
+    from morphompm import io as rio
+    from morphompm.state import ParticleState
+    from morphompm.config import SimConfig, Material
+    rng = np.random.default_rng(13)
+    n = 7
+    st = ParticleState(rng.standard_normal((n, 3)), rng.standard_normal((n, 3)), rng.standard_normal((n, 3, 3)),
+                       np.tile(np.eye(3), (n, 1, 1)) + 0.05 * rng.standard_normal((n, 3, 3)),
+                       np.tile(1.2 * np.eye(3), (n, 1, 1)))
+    st.x[0, 1] = -0.0          # formatting of signed zero
+    st.v[1, 2] = 1.0e-5        # and of an exponent
+    np.savez_compressed(os.path.join(HERE, "io_state.npz"), x=st.x, v=st.v, C=st.C, F=st.F, Fg=st.Fg)
+    rio.save_state(st, os.path.join(HERE, "io_state.csv"))
+    rio.save_state(st, os.path.join(HERE, "io_state.vtk"))
+    rio.save_config(SimConfig(N=12, dx=0.05, dt=2e-4, damping=0.07, sp=0.025,
+                              material=Material(E=3.0e3, nu=0.35, density=900.0)),
+                    os.path.join(HERE, "io_config.json"))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default=os.environ.get("MORPHOMPM_REF", "/root/reference"))
     ap.add_argument("--skip-c1", action="store_true")
+    ap.add_argument("--only", choices=["io"], default=None, help="write one group of fixtures")
     a = ap.parse_args()
+    if a.only == "io":
+        make_io(a.ref)
+        print("golden I/O fixtures written to", HERE)
+        return
     ref = _import_ref(a.ref)
     make_constitutive(ref)
     make_step(ref)
     make_gates(ref)
     if not a.skip_c1:
         make_c1_head(ref)
+    make_io(a.ref)
     print("golden fixtures written to", HERE)
 
 

@@ -177,3 +177,23 @@ def test_material_gradients_vs_fd_fp64(kind):
             fm, _ = integrate.dloss_dg(pts, cls(Material(**km)), cfg, 1.2, 5, True, loss=loss, x_obs=x_obs)
             fd = (fp - fm) / (2 * h)
             assert abs(grads[name] - fd) < 1e-6 * max(abs(fd), 1e-12) + 1e-14, (kind, loss, name, grads[name], fd)
+
+
+def test_save_batch_writes_each_scene(tmp_path):
+    from morphompm_b200 import io as mio, scenes
+    from morphompm_b200.batch import Batch, host_slab
+    sc = scenes.config4(seed=3, n_scenes=2, n_lo=300, n_hi=600)
+    b = Batch(sc, 3, dtype=torch.float32, active_cap=None)
+    b.load(host_slab(sc, np.float32), non_blocking=False)
+    b.rollout.forward(b.slab0)
+    paths = mio.save_batch(b, str(tmp_path / "scene{s}.npz"))
+    fin = b.rollout.final.double().cpu().numpy()
+    p0 = 0
+    for s, path in enumerate(paths):
+        st = mio.load_state(path)
+        k = st.n
+        assert k == sc[s]["x"].shape[0]
+        np.testing.assert_array_equal(st.x, fin[0:3, p0:p0 + k].T)
+        np.testing.assert_array_equal(st.F.reshape(k, 9), fin[15:24, p0:p0 + k].T)
+        assert np.allclose(st.Fg, (1.0 + sc[s]["growth_A"]) * np.eye(3))
+        p0 += k

@@ -41,6 +41,14 @@ void ref_set_growth(void* h, float g) {
     for (auto& p : static_cast<GrowthSolver*>(h)->particles()) p.Fg = Matrix3::scale(g, g, g);
 }
 
+// per-particle growth tensors, Fg (n x 3 x 3, row-major)
+void ref_set_growth_tensors(void* h, const float* Fg) {
+    auto& ps = static_cast<GrowthSolver*>(h)->particles();
+    for (size_t p = 0; p < ps.size(); ++p)
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) ps[p].Fg.m[i][j] = Fg[9 * p + 3 * i + j];
+}
+
 void ref_step(void* h, float dt, int steps) {
     GrowthSolver* s = static_cast<GrowthSolver*>(h);
     for (int t = 0; t < steps; ++t) s->step(dt);

@@ -27,6 +27,7 @@ def _load():
         lib.ref_destroy.argtypes = [vp]
         lib.ref_add.argtypes = [vp, ll, fp, f, f]
         lib.ref_set_growth.argtypes = [vp, f]
+        lib.ref_set_growth_tensors.argtypes = [vp, fp]
         lib.ref_step.argtypes = [vp, f, i]
         lib.ref_get.argtypes = [vp, fp, fp, fp, fp]
         _lib = lib
@@ -53,6 +54,10 @@ class RefSolver:
     def set_growth(self, g):
         self.lib.ref_set_growth(self.h, float(g))
 
+    def set_growth_tensors(self, Fg):
+        Fg = np.ascontiguousarray(Fg, dtype=np.float32).reshape(self.n, 3, 3)
+        self.lib.ref_set_growth_tensors(self.h, _fp(Fg))
+
     def step(self, dt, steps=1):
         self.lib.ref_step(self.h, float(dt), int(steps))
 
@@ -70,9 +75,26 @@ class RefSolver:
             self.h = None
 
 
+def blob(center, half, sp):
+    """Particles on the lattice of the reference's C++ tests: for each axis
+    c - h, c - h + sp, ... <= c + h + 1e-6, accumulated in single precision
+    as its loops do (test_growth.cpp:44-52, 123-127, 341-344)."""
+    c = np.broadcast_to(np.asarray(center, dtype=np.float64), 3)
+    h = np.broadcast_to(np.asarray(half, dtype=np.float64), 3)
+    axes = []
+    for d in range(3):
+        vals = []
+        lo, hi = np.float32(np.float32(c[d]) - np.float32(h[d])), np.float32(np.float32(c[d]) + np.float32(h[d]))
+        x = lo
+        while x <= np.float32(hi + np.float32(1e-6)):
+            vals.append(x)
+            x = np.float32(x + np.float32(sp))
+        axes.append(vals)
+    return np.array([(a, b, e) for a in axes[0] for b in axes[1] for e in axes[2]], dtype=np.float32)
+
+
 def parity_cube(sp=0.03, lo=0.27, hi=0.33):
-    """The 27-particle cube of the reference's parity scene, generated with the
-    same single-precision accumulation as its loop (test_growth.cpp:341-344)."""
+    """The 27-particle cube of the reference's parity scene (test_growth.cpp:341-344)."""
     pts = []
     x = np.float32(lo)
     while x <= np.float32(hi) + np.float32(1e-6):

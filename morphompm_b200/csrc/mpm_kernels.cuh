@@ -505,23 +505,42 @@ __device__ __forceinline__ void store_acc(R* __restrict__ S, long long cap, int 
             }
 }
 
+// OXB = 0: three lanes per cell, lane k sums the x-offset k (the three lanes
+// read the same records, one request per warp).
 template <typename R, int MODE, int OXB>
 __global__ void __launch_bounds__(128)
 cell_sums_kernel(Ctx ctx, const unsigned* __restrict__ perm, const R* __restrict__ payload, R* __restrict__ S,
                  long long cap) {
     const int nseg = *ctx.n_seg;
-    for (int id = blockIdx.x * blockDim.x + threadIdx.x; id < nseg; id += gridDim.x * blockDim.x) {
-        const int first = ctx.seg_first[id], last = ctx.seg_last[id];
-#pragma unroll 1
-        for (int ox0 = 0; ox0 < 3; ox0 += OXB) {
-            R acc[OXB][3][3][4];
-            zero_acc<R, OXB>(acc);
+    if constexpr (OXB == 0) {
+        const long long total = 3LL * nseg;
+        for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < total;
+             g += (long long)gridDim.x * blockDim.x) {
+            const int id = (int)(g / 3), ox0 = (int)(g % 3);
+            const int first = ctx.seg_first[id], last = ctx.seg_last[id];
+            R acc[1][3][3][4];
+            zero_acc<R, 1>(acc);
             for (int q = first; q < last; ++q) {
                 R r[PAYLOAD];
                 load_record(payload, perm[q], r);
-                accumulate_record<R, MODE, OXB>(r, ox0, acc);
+                accumulate_record<R, MODE, 1>(r, ox0, acc);
             }
-            store_acc<R, OXB>(S, cap, id, ox0, acc);
+            store_acc<R, 1>(S, cap, id, ox0, acc);
+        }
+    } else {
+        for (int id = blockIdx.x * blockDim.x + threadIdx.x; id < nseg; id += gridDim.x * blockDim.x) {
+            const int first = ctx.seg_first[id], last = ctx.seg_last[id];
+#pragma unroll 1
+            for (int ox0 = 0; ox0 < 3; ox0 += OXB) {
+                R acc[OXB][3][3][4];
+                zero_acc<R, OXB>(acc);
+                for (int q = first; q < last; ++q) {
+                    R r[PAYLOAD];
+                    load_record(payload, perm[q], r);
+                    accumulate_record<R, MODE, OXB>(r, ox0, acc);
+                }
+                store_acc<R, OXB>(S, cap, id, ox0, acc);
+            }
         }
     }
 }
@@ -532,87 +551,104 @@ cell_sums_kernel(Ctx ctx, const unsigned* __restrict__ perm, const R* __restrict
 // (advect) and Cn_b' = Cn_b + dt Fn_b F^T formed here from the cotangents of
 // the step's output, so no payload record is written for the reverse.
 // ---------------------------------------------------------------------------
+// the x-offsets ox_lo .. ox_lo + 3 - 1 of one occupied cell (OXB at a time)
+template <typename R, int OXB>
+__device__ __forceinline__ void adj_cell(const Ctx& ctx, const unsigned* __restrict__ perm, const MpmParticles& in,
+                                         const MpmCotangents& ob, R* __restrict__ S, long long cap, int advect,
+                                         int id, int ox_lo, int ox_hi) {
+    const int first = ctx.seg_first[id], last = ctx.seg_last[id];
+    const MpmScene& sc = ctx.scenes[ctx.scene_of[first]];
+    const R dx = (R)sc.dx, dt = (R)sc.dt, inv_dx = (R)(1.0 / sc.dx);
+    const R kdx = R(4) * inv_dx * inv_dx * dx;
+#pragma unroll 1
+    for (int ox0 = ox_lo; ox0 < ox_hi; ox0 += OXB) {
+        R acc[OXB][3][3][3];
+#pragma unroll
+        for (int a = 0; a < OXB; ++a)
+#pragma unroll
+            for (int b = 0; b < 3; ++b)
+#pragma unroll
+                for (int c = 0; c < 3; ++c)
+#pragma unroll
+                    for (int h = 0; h < 3; ++h) acc[a][b][c][h] = R(0);
+        for (int q = first; q < last; ++q) {
+            const long long p = perm[q];
+            R x[3], nv[3], B[9];
+            ld3<R>(in.x, p, in.sp3, in.sc3, x);
+            {
+                R F[9], Fb[9], Cb[9], xb[3];
+                ld9<R>(in.F, p, in.sp9, in.sc9, F);
+                ld9<R>(ob.F, p, ob.sp9, ob.sc9, Fb);
+                ld9<R>(ob.C, p, ob.sp9, ob.sc9, Cb);
+                ld3<R>(ob.v, p, ob.sp3, ob.sc3, nv);
+                if (advect) {
+                    ld3<R>(ob.x, p, ob.sp3, ob.sc3, xb);
+#pragma unroll
+                    for (int i = 0; i < 3; ++i) nv[i] += dt * xb[i];
+                }
+                R FbFt[9];
+                mmT(Fb, F, FbFt);
+#pragma unroll
+                for (int i = 0; i < 9; ++i) B[i] = kdx * (Cb[i] + dt * FbFt[i]);
+            }
+            int base[3];
+            R fx[3];
+            bin_particle(x, inv_dx, sc.shape, base, fx);
+            R w[3][3];
+            bspline(fx, w);
+            const R dz[3] = {R(0) - fx[2], R(1) - fx[2], R(2) - fx[2]};
+            const R dy[3] = {R(0) - fx[1], R(1) - fx[1], R(2) - fx[1]};
+#pragma unroll
+            for (int a = 0; a < OXB; ++a) {
+                const int ox = ox0 + a;
+                const R dpx = R(ox) - fx[0];
+                R wx;
+                if constexpr (OXB == 3) wx = w[a][0];
+                else wx = ox == 0 ? w[0][0] : (ox == 1 ? w[1][0] : w[2][0]);
+                const R ax0 = nv[0] + B[0] * dpx, ax1 = nv[1] + B[3] * dpx, ax2 = nv[2] + B[6] * dpx;
+#pragma unroll
+                for (int oy = 0; oy < 3; ++oy) {
+                    const R wxy = wx * w[oy][1];
+                    const R ay0 = ax0 + B[1] * dy[oy], ay1 = ax1 + B[4] * dy[oy], ay2 = ax2 + B[7] * dy[oy];
+#pragma unroll
+                    for (int oz = 0; oz < 3; ++oz) {
+                        const R wt = wxy * w[oz][2];
+                        acc[a][oy][oz][0] += wt * (ay0 + B[2] * dz[oz]);
+                        acc[a][oy][oz][1] += wt * (ay1 + B[5] * dz[oz]);
+                        acc[a][oy][oz][2] += wt * (ay2 + B[8] * dz[oz]);
+                    }
+                }
+            }
+        }
+#pragma unroll
+        for (int a = 0; a < OXB; ++a)
+#pragma unroll
+            for (int oy = 0; oy < 3; ++oy)
+#pragma unroll
+                for (int oz = 0; oz < 3; ++oz) {
+                    const int o = 9 * (ox0 + a) + 3 * oy + oz;
+                    const R v4[4] = {acc[a][oy][oz][0], acc[a][oy][oz][1], acc[a][oy][oz][2], R(0)};
+                    store_sum(S, (long long)o * cap + id, v4);
+                }
+    }
+}
+
+// OXB = 0: three lanes per cell, lane k sums the x-offset k.
 template <typename R, int OXB>
 __global__ void __launch_bounds__(128)
 cell_sums_adj_kernel(Ctx ctx, const unsigned* __restrict__ perm, MpmParticles in, MpmCotangents ob,
                      R* __restrict__ S, long long cap, int advect) {
     const int nseg = *ctx.n_seg;
-    for (int id = blockIdx.x * blockDim.x + threadIdx.x; id < nseg; id += gridDim.x * blockDim.x) {
-        const int first = ctx.seg_first[id], last = ctx.seg_last[id];
-        const MpmScene& sc = ctx.scenes[ctx.scene_of[first]];
-        const R dx = (R)sc.dx, dt = (R)sc.dt, inv_dx = (R)(1.0 / sc.dx);
-        const R kdx = R(4) * inv_dx * inv_dx * dx;
-#pragma unroll 1
-        for (int ox0 = 0; ox0 < 3; ox0 += OXB) {
-            R acc[OXB][3][3][3];
-#pragma unroll
-            for (int a = 0; a < OXB; ++a)
-#pragma unroll
-                for (int b = 0; b < 3; ++b)
-#pragma unroll
-                    for (int c = 0; c < 3; ++c)
-#pragma unroll
-                        for (int h = 0; h < 3; ++h) acc[a][b][c][h] = R(0);
-            for (int q = first; q < last; ++q) {
-                const long long p = perm[q];
-                R x[3], nv[3], B[9];
-                ld3<R>(in.x, p, in.sp3, in.sc3, x);
-                {
-                    R F[9], Fb[9], Cb[9], xb[3];
-                    ld9<R>(in.F, p, in.sp9, in.sc9, F);
-                    ld9<R>(ob.F, p, ob.sp9, ob.sc9, Fb);
-                    ld9<R>(ob.C, p, ob.sp9, ob.sc9, Cb);
-                    ld3<R>(ob.v, p, ob.sp3, ob.sc3, nv);
-                    if (advect) {
-                        ld3<R>(ob.x, p, ob.sp3, ob.sc3, xb);
-#pragma unroll
-                        for (int i = 0; i < 3; ++i) nv[i] += dt * xb[i];
-                    }
-                    R FbFt[9];
-                    mmT(Fb, F, FbFt);
-#pragma unroll
-                    for (int i = 0; i < 9; ++i) B[i] = kdx * (Cb[i] + dt * FbFt[i]);
-                }
-                int base[3];
-                R fx[3];
-                bin_particle(x, inv_dx, sc.shape, base, fx);
-                R w[3][3];
-                bspline(fx, w);
-                const R dz[3] = {R(0) - fx[2], R(1) - fx[2], R(2) - fx[2]};
-                const R dy[3] = {R(0) - fx[1], R(1) - fx[1], R(2) - fx[1]};
-#pragma unroll
-                for (int a = 0; a < OXB; ++a) {
-                    const int ox = ox0 + a;
-                    const R dpx = R(ox) - fx[0];
-                    R wx;
-                    if constexpr (OXB == 3) wx = w[a][0];
-                    else wx = ox == 0 ? w[0][0] : (ox == 1 ? w[1][0] : w[2][0]);
-                    const R ax0 = nv[0] + B[0] * dpx, ax1 = nv[1] + B[3] * dpx, ax2 = nv[2] + B[6] * dpx;
-#pragma unroll
-                    for (int oy = 0; oy < 3; ++oy) {
-                        const R wxy = wx * w[oy][1];
-                        const R ay0 = ax0 + B[1] * dy[oy], ay1 = ax1 + B[4] * dy[oy], ay2 = ax2 + B[7] * dy[oy];
-#pragma unroll
-                        for (int oz = 0; oz < 3; ++oz) {
-                            const R wt = wxy * w[oz][2];
-                            acc[a][oy][oz][0] += wt * (ay0 + B[2] * dz[oz]);
-                            acc[a][oy][oz][1] += wt * (ay1 + B[5] * dz[oz]);
-                            acc[a][oy][oz][2] += wt * (ay2 + B[8] * dz[oz]);
-                        }
-                    }
-                }
-            }
-#pragma unroll
-            for (int a = 0; a < OXB; ++a)
-#pragma unroll
-                for (int oy = 0; oy < 3; ++oy)
-#pragma unroll
-                    for (int oz = 0; oz < 3; ++oz) {
-                        const int o = 9 * (ox0 + a) + 3 * oy + oz;
-                        const R v4[4] = {acc[a][oy][oz][0], acc[a][oy][oz][1], acc[a][oy][oz][2], R(0)};
-                        store_sum(S, (long long)o * cap + id, v4);
-                    }
+    if constexpr (OXB == 0) {
+        const long long total = 3LL * nseg;
+        for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < total;
+             g += (long long)gridDim.x * blockDim.x) {
+            const int ox = (int)(g % 3);
+            adj_cell<R, 1>(ctx, perm, in, ob, S, cap, advect, (int)(g / 3), ox, ox + 1);
         }
+    } else {
+        for (int id = blockIdx.x * blockDim.x + threadIdx.x; id < nseg; id += gridDim.x * blockDim.x)
+            adj_cell<R, OXB>(ctx, perm, in, ob, S, cap, advect, id, 0, 3);
     }
 }
 

@@ -151,6 +151,13 @@ int64_t mpm_plan_launch_count(const MpmPlan* plan);
  * reference (its scene parameters are Python objects rebuilt per call). */
 int mpm_plan_update_scenes(MpmPlan* plan, const MpmScene* scenes, int32_t n_scenes, void* stream);
 
+/* Optional per-particle mass and reference volume (real type, n entries in
+ * particle order, in place of the scene's pmass / vol0; either may be NULL),
+ * as the reference's C++ Particle carries them (growth_solver.h:31-39).
+ * The arrays must stay valid while the plan is used.  Ends any chain of
+ * mpm_step_fwd_chain calls. */
+int mpm_plan_set_particle_mass(MpmPlan* plan, const void* mass, const void* vol0);
+
 /* Optional per-particle growth field phi_p (growth_mode 1), real type. */
 int mpm_plan_set_growth_field(MpmPlan* plan, const void* phi);
 

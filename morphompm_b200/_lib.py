@@ -72,6 +72,7 @@ EXPORTS = {
     "mpm_plan_read_status": (i32, [vp, C.POINTER(i32), vp]),
     "mpm_plan_read_fp64_fallbacks": (i32, [vp, C.POINTER(i64), vp]),
     "mpm_plan_set_growth_field": (i32, [vp, vp]),
+    "mpm_plan_set_particle_mass": (i32, [vp, vp, vp]),
     "mpm_plan_profile_begin": (i32, [vp, C.c_uint32, i32]),
     "mpm_plan_profile_end": (i32, [vp, C.POINTER(f64), C.POINTER(i32)]),
     "mpm_plan_launch_count": (i64, [vp]),

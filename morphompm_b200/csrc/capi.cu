@@ -61,6 +61,8 @@ struct MpmPlan {
     size_t t_skeys, t_perm, t_seg_first, t_seg_last, t_nseg, t_active, t_nact, t_grid, tape_bytes = 0;
     char* ws = nullptr;
     const void* phi = nullptr;
+    const void* pmass_p = nullptr;     // per-particle masses / reference volumes (optional)
+    const void* vol0_p = nullptr;
     int n_sm = 148;
     // profiling
     uint32_t prof_mask = 0;
@@ -90,6 +92,8 @@ Ctx make_ctx(MpmPlan* P) {
     c.blk_count = at<unsigned>(P, P->o_blk);
     c.tile_flag = at<int>(P, P->o_tile_flag);
     c.phi = P->phi;
+    c.pmass_p = P->pmass_p;
+    c.vol0_p = P->vol0_p;
     c.dense_f = P->ws + P->o_dense_f;
     c.dense_b = P->ws + P->o_dense_b;
     c.n = P->n;
@@ -570,6 +574,14 @@ int mpm_plan_update_scenes(MpmPlan* P, const MpmScene* scenes, int32_t n_scenes,
                         cudaMemcpyHostToDevice, st) != cudaSuccess ||
         cudaStreamSynchronize(st) != cudaSuccess)
         return MPM_ERR_CUDA;
+    return MPM_OK;
+}
+
+int mpm_plan_set_particle_mass(MpmPlan* P, const void* mass, const void* vol0) {
+    if (!P) return MPM_ERR_ARG;
+    P->pmass_p = mass;
+    P->vol0_p = vol0;
+    P->chain_valid = false;     // records formed with the old masses
     return MPM_OK;
 }
 

@@ -38,6 +38,8 @@ struct Ctx {
     unsigned* blk_count;         // per-block segment counts of the segment scan
     int* tile_flag;              // 1 if the tile receives mass this step
     const void* phi;             // growth field phi_p (growth_mode 1), may be null
+    const void* pmass_p;         // per-particle mass, may be null (scene pmass)
+    const void* vol0_p;          // per-particle reference volume, may be null (scene vol0)
     void* dense_f;               // dense node scratch, forward record (m, v[3]) per node
     void* dense_b;               // dense node scratch, reverse record (gm_b, gmom_b[3]) per node
     long long n;
@@ -246,6 +248,14 @@ __device__ __forceinline__ void bspline_grad(const R fx[3], R dw[3][3]) {
         dw[1][d] = R(-2.0) * (fx[d] - R(1.0));
         dw[2][d] = fx[d] - R(0.5);
     }
+}
+
+// mass and reference volume of particle p: per particle when the plan has
+// them, else the scene's
+template <typename R>
+__device__ __forceinline__ void particle_mass(const Ctx& ctx, const MpmScene& sc, long long p, R& pm, R& vol0) {
+    pm = ctx.pmass_p ? static_cast<const R*>(ctx.pmass_p)[p] : (R)sc.pmass;
+    vol0 = ctx.vol0_p ? static_cast<const R*>(ctx.vol0_p)[p] : (R)sc.vol0;
 }
 
 __device__ __forceinline__ void raise_status(int* status, int bits) {

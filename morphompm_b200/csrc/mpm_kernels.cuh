@@ -379,8 +379,9 @@ seg_write_kernel(Ctx ctx, const unsigned* __restrict__ skeys) {
 // record: fx[0..2], pmass, a = pmass v, B = (pmass C + dt sk) dx
 // ---------------------------------------------------------------------------
 template <typename R>
-__device__ __forceinline__ void p2g_record(const Ctx& ctx, const MpmScene& sc, const R fx[3], const R v[3],
-                                           const R C[9], const R F[9], const R Fg[9], R rec[PAYLOAD]) {
+__device__ __forceinline__ void p2g_record(const Ctx& ctx, const MpmScene& sc, long long p, const R fx[3],
+                                           const R v[3], const R C[9], const R F[9], const R Fg[9],
+                                           R rec[PAYLOAD]) {
     ModelParams<R> M;
     M.load(sc);
     const R dx = (R)sc.dx, dt = (R)sc.dt, inv_dx = (R)(1.0 / sc.dx);
@@ -388,8 +389,9 @@ __device__ __forceinline__ void p2g_record(const Ctx& ctx, const MpmScene& sc, c
     R tau[9];
     bool fb = model_stress(M, ctx.gap_thresh, F, Fg, C, tau);
     if (fb) atomicAdd(ctx.fallbacks, 1ull);
-    R c = -k4 * (R)sc.vol0 * det3(Fg);
-    const R pm = (R)sc.pmass;
+    R pm, vol0;
+    particle_mass<R>(ctx, sc, p, pm, vol0);
+    R c = -k4 * vol0 * det3(Fg);
     rec[0] = fx[0]; rec[1] = fx[1]; rec[2] = fx[2]; rec[3] = pm;
 #pragma unroll
     for (int i = 0; i < 3; ++i) rec[4 + i] = pm * v[i];
@@ -414,7 +416,7 @@ prepass_kernel(Ctx ctx, MpmParticles P, R* __restrict__ payload, int t) {
     R fx[3];
     bin_particle(x, (R)(1.0 / sc.dx), sc.shape, base, fx);
     R rec[PAYLOAD];
-    p2g_record<R>(ctx, sc, fx, v, C, F, Fg, rec);
+    p2g_record<R>(ctx, sc, p, fx, v, C, F, Fg, rec);
     store_record(payload, p, rec);
 }
 
@@ -871,7 +873,7 @@ g2p_kernel(Ctx ctx, Tape<R> tp, MpmParticles in, MpmParticles out, int advect, u
         R fxn[3], Fg[9], rec[PAYLOAD];
         keys[p] = particle_key<R>(ctx, sc, ax, xn, fxn);
         load_Fg<R>(ctx, sc, in, p, t + 1, Fg, nullptr);
-        p2g_record<R>(ctx, sc, fxn, nv, nC, Fn, Fg, rec);
+        p2g_record<R>(ctx, sc, p, fxn, nv, nC, Fn, Fg, rec);
         store_record(payload, p, rec);
     }
 }
@@ -900,7 +902,8 @@ bwd_particle_kernel(Ctx ctx, Tape<R> tp, MpmParticles in, const R* __restrict__ 
     M.load(sc);
     const R dx = (R)sc.dx, dt = (R)sc.dt, inv_dx = (R)(1.0 / sc.dx);
     const R k4 = R(4) * inv_dx * inv_dx;
-    const R pm = (R)sc.pmass;
+    R pm, vol0;
+    particle_mass<R>(ctx, sc, p, pm, vol0);
     R x[3], C[9], F[9], Fg[9];
     R gphi;
     ld3<R>(in.x, p, in.sp3, in.sc3, x);
@@ -915,7 +918,7 @@ bwd_particle_kernel(Ctx ctx, Tape<R> tp, MpmParticles in, const R* __restrict__ 
     __shared__ R keep_s[13][256];
 #pragma unroll
     for (int i = 0; i < 13; ++i) keep_s[i][threadIdx.x] = keep[i];
-    const R c = -k4 * (R)sc.vol0 * det3(Fg);
+    const R c = -k4 * vol0 * det3(Fg);
 
     // per-particle matrices of the regrouped x_b terms
     R M1[9], M2[9], nvb[3], pv[3];
@@ -1080,7 +1083,7 @@ bwd_particle_kernel(Ctx ctx, Tape<R> tp, MpmParticles in, const R* __restrict__ 
     // volume path: c = -k4 vol0 det(Fg)
     R Fgi[9];
     R dFg = inv3(Fg, Fgi);
-    R vol = frob(skb, tau) * (-k4 * (R)sc.vol0) * dFg;
+    R vol = frob(skb, tau) * (-k4 * vol0) * dFg;
     double Fgl[9];
 #pragma unroll
     for (int i = 0; i < 3; ++i)

@@ -163,6 +163,17 @@ class Plan:
         self.scenes = scenes
         self._c_scenes = arr
 
+    def set_particle_mass(self, mass: Optional[torch.Tensor], vol0: Optional[torch.Tensor] = None):
+        """Per-particle masses and reference volumes (None: the scenes' pmass / vol0)."""
+        prep = lambda a: (a.to(device=self.device, dtype=self.dtype).contiguous() if a is not None else None)
+        mass, vol0 = prep(mass), prep(vol0)
+        for a in (mass, vol0):
+            assert a is None or a.numel() == self.n
+        self._mass = (mass, vol0)     # kept alive while the plan uses them
+        L.check(self.lib.mpm_plan_set_particle_mass(
+            self.handle, C.c_void_p(mass.data_ptr() if mass is not None else 0),
+            C.c_void_p(vol0.data_ptr() if vol0 is not None else 0)), "set_particle_mass")
+
     def set_growth_field(self, phi: Optional[torch.Tensor]):
         if phi is not None:
             phi = phi.to(device=self.device, dtype=self.dtype).contiguous()

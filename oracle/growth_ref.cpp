@@ -36,6 +36,13 @@ void ref_add(void* h, long long n, const float* x, float mass, float density) {
     for (long long p = 0; p < n; ++p) s->add_particle(Vec3(x[3 * p], x[3 * p + 1], x[3 * p + 2]), mass, density);
 }
 
+// n particles, each with its own mass and density (vol0 = mass / density)
+void ref_add_each(void* h, long long n, const float* x, const float* mass, const float* density) {
+    GrowthSolver* s = static_cast<GrowthSolver*>(h);
+    for (long long p = 0; p < n; ++p)
+        s->add_particle(Vec3(x[3 * p], x[3 * p + 1], x[3 * p + 2]), mass[p], density[p]);
+}
+
 // Fg = g I for every particle
 void ref_set_growth(void* h, float g) {
     for (auto& p : static_cast<GrowthSolver*>(h)->particles()) p.Fg = Matrix3::scale(g, g, g);

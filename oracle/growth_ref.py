@@ -26,6 +26,7 @@ def _load():
         lib.ref_create.argtypes = [i, f, f, f, f, f, f, f]
         lib.ref_destroy.argtypes = [vp]
         lib.ref_add.argtypes = [vp, ll, fp, f, f]
+        lib.ref_add_each.argtypes = [vp, ll, fp, fp, fp]
         lib.ref_set_growth.argtypes = [vp, f]
         lib.ref_set_growth_tensors.argtypes = [vp, fp]
         lib.ref_step.argtypes = [vp, f, i]
@@ -49,6 +50,13 @@ class RefSolver:
     def add(self, x, mass, density):
         x = np.ascontiguousarray(x, dtype=np.float32)
         self.lib.ref_add(self.h, x.shape[0], _fp(x), float(mass), float(density))
+        self.n += x.shape[0]
+
+    def add_each(self, x, mass, density):
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        m = np.ascontiguousarray(mass, dtype=np.float32)
+        d = np.ascontiguousarray(density, dtype=np.float32)
+        self.lib.ref_add_each(self.h, x.shape[0], _fp(x), _fp(m), _fp(d))
         self.n += x.shape[0]
 
     def set_growth(self, g):

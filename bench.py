@@ -203,7 +203,7 @@ def run_reference(a):
             break
         jobs.append((scn[i], steps))
         acc += u
-    vals = []
+    vals, wall = [], []
     with ctx.Pool(cores) as pool:
         for it in range(a.warmup + a.steps):
             t0 = time.perf_counter()
@@ -211,9 +211,10 @@ def run_reference(a):
             dt = time.perf_counter() - t0
             if it >= a.warmup:
                 vals.append(sum(u for u, _ in res) / dt)
+                wall.append(dt * 1e3)
     v = float(np.median(vals))
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": a.gpus, "steps": a.steps,
-            "warmup": a.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+            "warmup": a.warmup, "ms_per_step": float(np.median(wall)), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": WORKLOAD, "scenes": a.scenes, "mpm_steps": a.mpm_steps},
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port",

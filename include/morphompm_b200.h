@@ -36,6 +36,7 @@ extern "C" {
 #define MPM_MODEL_NEOHOOKEAN        0   /* constitutive.py:25-39  */
 #define MPM_MODEL_HENCKY            1   /* constitutive.py:42-75  */
 #define MPM_MODEL_HERSCHEL_BULKLEY  2   /* constitutive.py:106-147 */
+#define MPM_MODEL_EXTERNAL          3   /* stress supplied by the caller (mpm_plan_set_external_stress) */
 
 /* ---- kernel kinds (for mpm_plan_profile_begin) ---- */
 #define MPM_K_BIN           0   /* cell keys                                 */
@@ -150,6 +151,19 @@ int64_t mpm_plan_launch_count(const MpmPlan* plan);
  * mpm_step_fwd_chain calls.  Synchronises `stream`.  No counterpart in the
  * reference (its scene parameters are Python objects rebuilt per call). */
 int mpm_plan_update_scenes(MpmPlan* plan, const MpmScene* scenes, int32_t n_scenes, void* stream);
+
+/* Stress supplied by the caller for scenes of kind MPM_MODEL_EXTERNAL (a
+ * material defined outside this library, evaluated by the caller before the
+ * step): tau is the Kirchhoff stress of every particle, n x 3 x 3 row-major,
+ * real type, in particle order.  mpm_step_fwd uses it in place of a built-in
+ * model; mpm_step_bwd writes the cotangent of that stress to tau_bar (same
+ * layout) and leaves the stress's own VJP (its F, Fg and C cotangents) to the
+ * caller, who adds them.  The device counterpart of the reference's seam,
+ * which takes any material object with stress / stress_vjp (constitutive.py:
+ * 3-5, 79-103).  Both buffers must stay valid while the steps run; a plan with an
+ * external scene refuses chained steps and, without tau (tau_bar in the
+ * reverse), returns MPM_ERR_ARG. */
+int mpm_plan_set_external_stress(MpmPlan* plan, const void* tau, void* tau_bar);
 
 /* Optional per-particle mass and reference volume (real type, n entries in
  * particle order, in place of the scene's pmass / vol0; either may be NULL),

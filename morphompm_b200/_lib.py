@@ -27,6 +27,7 @@ KERNELS = ["bin", "sort", "mark", "compact", "prepass", "p2g", "g2p", "bwd_paylo
 
 MODEL_NEOHOOKEAN = 0
 MODEL_HENCKY = 1
+MODEL_EXTERNAL = 3
 MODEL_HERSCHEL_BULKLEY = 2
 
 i32, i64, f32, f64, vp = C.c_int32, C.c_int64, C.c_float, C.c_double, C.c_void_p
@@ -73,6 +74,7 @@ EXPORTS = {
     "mpm_plan_read_fp64_fallbacks": (i32, [vp, C.POINTER(i64), vp]),
     "mpm_plan_set_growth_field": (i32, [vp, vp]),
     "mpm_plan_set_particle_mass": (i32, [vp, vp, vp]),
+    "mpm_plan_set_external_stress": (i32, [vp, vp, vp]),
     "mpm_plan_profile_begin": (i32, [vp, C.c_uint32, i32]),
     "mpm_plan_profile_end": (i32, [vp, C.POINTER(f64), C.POINTER(i32)]),
     "mpm_plan_launch_count": (i64, [vp]),

@@ -109,10 +109,51 @@ class HerschelBulkley(_Model):
                                              m=self.m, eps=self.eps))
 
 
+def is_external(model) -> bool:
+    """A user-defined material: not built in, but with batched
+    ``stress(F, Fg, C) -> tau`` and ``stress_vjp(F, Fg, C, tau_bar) ->
+    (F_bar, Fg_bar, C_bar)`` on (n, 3, 3) device tensors."""
+    return (not isinstance(model, _Model) and callable(getattr(model, "stress", None))
+            and callable(getattr(model, "stress_vjp", None)))
+
+
 def model_fields(model) -> dict:
-    """Scene fields of a built-in model; anything else is rejected (the GPU
-    path has no CPU fallback for a Python-defined material)."""
+    """Scene fields of a model.  A built-in model runs inside the kernels; a
+    user-defined one (``is_external``) runs as a batched callback whose stress
+    the kernels consume (``transfer.step`` / ``step_vjp`` only).  Anything
+    else is rejected: the GPU path has no CPU fallback."""
     if isinstance(model, _Model):
         return model.scene_fields()
-    raise TypeError(f"{type(model).__name__} is not a built-in morphompm_b200 model "
-                    "(NeoHookean, Hencky, HerschelBulkley)")
+    if is_external(model):
+        return dict(model=L.MODEL_EXTERNAL)
+    raise TypeError(f"{type(model).__name__} is not a morphompm_b200 model: use NeoHookean, Hencky, "
+                    "HerschelBulkley, or an object with batched stress(F, Fg, C) and stress_vjp(F, Fg, C, tau_bar)")
+
+
+class PerParticle:
+    """Batched adapter for a material written like the reference's models
+    (constitutive.py:3-5: ``stress`` and ``stress_vjp`` on one particle's
+    3x3 numpy arrays).  It loops over the particles on the host, so it is
+    slow; it lets such a material run unchanged through ``transfer.step``."""
+
+    def __init__(self, model):
+        self.model = model
+
+    @staticmethod
+    def _np(a):
+        return a.detach().double().cpu().numpy() if hasattr(a, "detach") else np.asarray(a, dtype=np.float64)
+
+    def stress(self, F, Fg, C=None):
+        import torch
+        Fh, Fgh = self._np(F), self._np(Fg)
+        Ch = self._np(C) if C is not None else np.zeros_like(Fh)
+        tau = np.stack([np.asarray(self.model.stress(Fh[p], Fgh[p], Ch[p])) for p in range(Fh.shape[0])])
+        return torch.as_tensor(tau, dtype=F.dtype, device=F.device)
+
+    def stress_vjp(self, F, Fg, C, tau_bar):
+        import torch
+        Fh, Fgh, tb = self._np(F), self._np(Fg), self._np(tau_bar)
+        Ch = self._np(C) if C is not None else np.zeros_like(Fh)
+        outs = [self.model.stress_vjp(Fh[p], Fgh[p], Ch[p], tb[p]) for p in range(Fh.shape[0])]
+        return tuple(torch.as_tensor(np.stack([o[k] for o in outs]), dtype=F.dtype, device=F.device)
+                     for k in range(3))

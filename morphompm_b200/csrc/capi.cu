@@ -63,6 +63,9 @@ struct MpmPlan {
     const void* phi = nullptr;
     const void* pmass_p = nullptr;     // per-particle masses / reference volumes (optional)
     const void* vol0_p = nullptr;
+    const void* ext_tau = nullptr;     // caller-supplied stress and its cotangent (MPM_MODEL_EXTERNAL)
+    void* ext_tau_bar = nullptr;
+    bool any_external = false;
     int n_sm = 148;
     // profiling
     uint32_t prof_mask = 0;
@@ -94,6 +97,8 @@ Ctx make_ctx(MpmPlan* P) {
     c.phi = P->phi;
     c.pmass_p = P->pmass_p;
     c.vol0_p = P->vol0_p;
+    c.ext_tau = P->ext_tau;
+    c.ext_tau_bar = P->ext_tau_bar;
     c.dense_f = P->ws + P->o_dense_f;
     c.dense_b = P->ws + P->o_dense_b;
     c.n = P->n;
@@ -325,12 +330,18 @@ int step_bwd_R(MpmPlan* P, const MpmParticles& in, const void* outC, const MpmCo
     double* dmat = dbuf + P->n;     // material gradients per slot: mu, then lambda
     {
         Site s(P, MPM_K_BWD_PARTICLE, 1, st);
-        if (material_grad)
-            bwd_particle_kernel<R, true><<<g, B, 0, st>>>(ctx, tp, in, static_cast<const R*>(outC), ob, ib,
-                                                          want_dA ? dbuf : nullptr, dmat, advect, t);
-        else
-            bwd_particle_kernel<R, false><<<g, B, 0, st>>>(ctx, tp, in, static_cast<const R*>(outC), ob, ib,
-                                                           want_dA ? dbuf : nullptr, nullptr, advect, t);
+        const R* oC = static_cast<const R*>(outC);
+        double* dAp = want_dA ? dbuf : nullptr;
+        if (P->any_external) {
+            if (material_grad)
+                bwd_particle_kernel<R, true, true><<<g, B, 0, st>>>(ctx, tp, in, oC, ob, ib, dAp, dmat, advect, t);
+            else
+                bwd_particle_kernel<R, false, true><<<g, B, 0, st>>>(ctx, tp, in, oC, ob, ib, dAp, nullptr, advect, t);
+        } else if (material_grad) {
+            bwd_particle_kernel<R, true, false><<<g, B, 0, st>>>(ctx, tp, in, oC, ob, ib, dAp, dmat, advect, t);
+        } else {
+            bwd_particle_kernel<R, false, false><<<g, B, 0, st>>>(ctx, tp, in, oC, ob, ib, dAp, nullptr, advect, t);
+        }
     }
     if (want_dA) {
         Site s(P, MPM_K_REDUCE, 1, st);
@@ -348,7 +359,7 @@ int step_bwd_R(MpmPlan* P, const MpmParticles& in, const void* outC, const MpmCo
 bool scene_ok(const MpmScene& s) {
     for (int d = 0; d < 3; ++d)
         if (s.shape[d] < 1 || s.shape[d] > 4096) return false;
-    if (s.model < 0 || s.model > 2) return false;
+    if (s.model < 0 || s.model > MPM_MODEL_EXTERNAL) return false;
     if (!(s.dx > 0) || !(s.dt >= 0)) return false;
     if (s.p_end < s.p_begin) return false;
     return true;
@@ -396,6 +407,7 @@ int mpm_plan_create(const MpmScene* scenes, int32_t n_scenes, int32_t real_bytes
         P->scenes.push_back(sc);
         P->aux.push_back(a);
         if (sc.growth_mode == 1) P->any_growth = true;
+        if (sc.model == MPM_MODEL_EXTERNAL) P->any_external = true;
         for (long long p = sc.p_begin; p < sc.p_end; ++p) P->scene_of.push_back(s);
         for (long long k = a.tile_begin; k < tile; ++k) P->tile_scene.push_back(s);
     }
@@ -577,6 +589,14 @@ int mpm_plan_update_scenes(MpmPlan* P, const MpmScene* scenes, int32_t n_scenes,
     return MPM_OK;
 }
 
+int mpm_plan_set_external_stress(MpmPlan* P, const void* tau, void* tau_bar) {
+    if (!P) return MPM_ERR_ARG;
+    P->ext_tau = tau;
+    P->ext_tau_bar = tau_bar;
+    P->chain_valid = false;
+    return MPM_OK;
+}
+
 int mpm_plan_set_particle_mass(MpmPlan* P, const void* mass, const void* vol0) {
     if (!P) return MPM_ERR_ARG;
     P->pmass_p = mass;
@@ -600,6 +620,9 @@ int mpm_step_fwd_chain(MpmPlan* P, const MpmParticles* in, MpmParticles* out, in
         if (s.growth_mode == 0 && !in->Fg) return MPM_ERR_ARG;
     char* tp = tape ? static_cast<char*>(tape) : P->ws + P->o_tape;
     if (reinterpret_cast<uintptr_t>(tp) % ALIGN) return MPM_ERR_ARG;
+    // external stress: supplied per call, so no chaining (the chain would
+    // evaluate the next step's stress inside G2P)
+    if (P->any_external && (!P->ext_tau || flags != 0)) return MPM_ERR_ARG;
     // a chained step must continue the last emitting call on this plan
     if (flags & MPM_FWD_CHAINED) {
         if (!P->chain_valid || P->chain_t != step_index ||
@@ -634,6 +657,7 @@ int mpm_step_bwd_params(MpmPlan* P, const MpmParticles* in, const void* out_C, c
         return MPM_ERR_ARG;
     for (const MpmScene& s : P->scenes)
         if (s.growth_mode == 0 && !in->Fg) return MPM_ERR_ARG;
+    if (P->any_external && (!P->ext_tau || !P->ext_tau_bar)) return MPM_ERR_ARG;
     if (reinterpret_cast<uintptr_t>(tape) % ALIGN) return MPM_ERR_ARG;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     return P->real_bytes == 4
@@ -653,6 +677,7 @@ int mpm_step_bwd(MpmPlan* P, const MpmParticles* in, const void* out_C, const Mp
 int mpm_stress(const MpmScene* scene, int32_t real_bytes, int64_t n, const void* F, const void* Fg, const void* C,
                void* tau, void* stream) {
     if (!scene || n < 0 || !F || !Fg || !tau || (real_bytes != 4 && real_bytes != 8)) return MPM_ERR_ARG;
+    if (scene->model == MPM_MODEL_EXTERNAL) return MPM_ERR_UNSUPPORTED;
     if (n == 0) return MPM_OK;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     int g = grid_for(n, 256);
@@ -669,6 +694,7 @@ int mpm_stress_vjp(const MpmScene* scene, int32_t real_bytes, int64_t n, const v
                    const void* C, const void* tau_bar, void* F_bar, void* Fg_bar, void* C_bar, void* stream) {
     if (!scene || n < 0 || !F || !Fg || !tau_bar || !F_bar || !Fg_bar || (real_bytes != 4 && real_bytes != 8))
         return MPM_ERR_ARG;
+    if (scene->model == MPM_MODEL_EXTERNAL) return MPM_ERR_UNSUPPORTED;
     if (n == 0) return MPM_OK;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     int g = grid_for(n, 256);
@@ -844,6 +870,7 @@ extern "C" int mpm_step_fwd_noalloc(const MpmScene* scene, int32_t real_bytes, c
     if (!scene || !in || !out || (real_bytes != 4 && real_bytes != 8)) return MPM_ERR_ARG;
     if (!scene_ok(*scene) || scene->p_begin != 0 || scene->p_end < 1 || scene->p_end >= (1LL << 31))
         return MPM_ERR_ARG;
+    if (scene->model == MPM_MODEL_EXTERNAL) return MPM_ERR_UNSUPPORTED;
     if (!in->x || !in->v || !in->C || !in->F || !out->x || !out->v || !out->C || !out->F || in->x == out->x ||
         in->F == out->F || (scene->growth_mode == 0 && !in->Fg))
         return MPM_ERR_ARG;

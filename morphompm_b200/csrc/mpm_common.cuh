@@ -40,6 +40,8 @@ struct Ctx {
     const void* phi;             // growth field phi_p (growth_mode 1), may be null
     const void* pmass_p;         // per-particle mass, may be null (scene pmass)
     const void* vol0_p;          // per-particle reference volume, may be null (scene vol0)
+    const void* ext_tau;         // MPM_MODEL_EXTERNAL scenes: Kirchhoff stress per particle (n x 9)
+    void* ext_tau_bar;           // and its cotangent, written by the reverse step (n x 9)
     void* dense_f;               // dense node scratch, forward record (m, v[3]) per node
     void* dense_b;               // dense node scratch, reverse record (gm_b, gmom_b[3]) per node
     long long n;

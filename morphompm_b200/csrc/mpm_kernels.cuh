@@ -387,7 +387,11 @@ __device__ __forceinline__ void p2g_record(const Ctx& ctx, const MpmScene& sc, l
     const R dx = (R)sc.dx, dt = (R)sc.dt, inv_dx = (R)(1.0 / sc.dx);
     const R k4 = R(4) * inv_dx * inv_dx;
     R tau[9];
-    bool fb = model_stress(M, ctx.gap_thresh, F, Fg, C, tau);
+    bool fb = false;
+    if (M.kind == MPM_MODEL_EXTERNAL)
+        ld9<R>(ctx.ext_tau, p, 9, 1, tau);      // the caller's stress
+    else
+        fb = model_stress(M, ctx.gap_thresh, F, Fg, C, tau);
     if (fb) atomicAdd(ctx.fallbacks, 1ull);
     R pm, vol0;
     particle_mass<R>(ctx, sc, p, pm, vol0);
@@ -886,8 +890,8 @@ g2p_kernel(Ctx ctx, Tape<R> tp, MpmParticles in, MpmParticles out, int advect, u
 // summed once per particle: x_b -= M1 sum(w gv) + M2 sum(w mb).
 // ---------------------------------------------------------------------------
 // MAT: also the material-parameter gradients per slot, dmat[sidx] (mu) and
-// dmat[n + sidx] (lambda).
-template <typename R, bool MAT>
+// dmat[n + sidx] (lambda).  EXT: the plan has MPM_MODEL_EXTERNAL scenes.
+template <typename R, bool MAT, bool EXT>
 __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 2 : 1)
 bwd_particle_kernel(Ctx ctx, Tape<R> tp, MpmParticles in, const R* __restrict__ outC,
                     MpmCotangents ob, MpmCotangents ib, double* __restrict__ dA, double* __restrict__ dmat,
@@ -912,7 +916,11 @@ bwd_particle_kernel(Ctx ctx, Tape<R> tp, MpmParticles in, const R* __restrict__ 
     load_Fg<R>(ctx, sc, in, p, t, Fg, &gphi);
 
     R tau[9], keep[13];
-    bool fb = model_stress_keep(M, ctx.gap_thresh, F, Fg, C, tau, keep);
+    bool fb = false;
+    if (EXT && M.kind == MPM_MODEL_EXTERNAL)
+        ld9<R>(ctx.ext_tau, p, 9, 1, tau);      // the caller's stress
+    else
+        fb = model_stress_keep(M, ctx.gap_thresh, F, Fg, C, tau, keep);
     // the kept eigendecomposition waits in shared memory (one column per
     // thread) while the node loop holds the registers
     __shared__ R keep_s[13][256];
@@ -1067,7 +1075,14 @@ bwd_particle_kernel(Ctx ctx, Tape<R> tp, MpmParticles in, const R* __restrict__ 
 #pragma unroll
         for (int i = 0; i < 13; ++i) keep[i] = ks[i * 256];
     }
-    fb |= model_vjp_keep(M, ctx.gap_thresh, F, Fg, C, taub, keep, Fb2, Fgb, Cb2);
+    if (EXT && M.kind == MPM_MODEL_EXTERNAL) {
+        // the caller applies its own stress VJP to tau_bar
+        st9<R>(ctx.ext_tau_bar, p, 9, 1, taub);
+#pragma unroll
+        for (int i = 0; i < 9; ++i) Fb2[i] = Fgb[i] = Cb2[i] = R(0);
+    } else {
+        fb |= model_vjp_keep(M, ctx.gap_thresh, F, Fg, C, taub, keep, Fb2, Fgb, Cb2);
+    }
     if (fb) atomicAdd(ctx.fallbacks, 1ull);
     if constexpr (MAT) {
         double gm[2];

@@ -23,6 +23,7 @@ import torch
 from .devarray import like_input, to_device
 from .runtime import SLAB_ROWS, ROW_C, ROW_F, ROW_V, ROW_X
 from .state import ParticleState
+from .constitutive import is_external
 from .transfer import get_plan, scene_spec, step, step_vjp
 
 
@@ -95,6 +96,8 @@ def dloss_dg(pts, model, cfg, g, n_steps, advect, loss: str = "detF", x_obs=None
     loss="detF": sum det F_final (the reference's); loss="mse": mean
     |x_final - x_obs|^2."""
     from .trajectory import Rollout
+    if is_external(model):
+        return _dloss_dg_steps(pts, model, cfg, g, n_steps, advect, loss, x_obs)
     p = to_device(pts).contiguous()
     n = p.shape[0]
     plan = get_plan([scene_spec(cfg, model, n)], p.dtype, p.device)
@@ -110,6 +113,32 @@ def dloss_dg(pts, model, cfg, g, n_steps, advect, loss: str = "detF", x_obs=None
     L = float(ro.loss.sum().item())
     dg = float(ro.Fg_bar[0].sum().item() + ro.Fg_bar[4].sum().item() + ro.Fg_bar[8].sum().item())
     return L, dg
+
+
+def _dloss_dg_steps(pts, model, cfg, g, n_steps, advect, loss, x_obs):
+    """dloss_dg through the single-step API (per-step caches, as the
+    reference's rollout / rollout_vjp): the path of user-defined materials,
+    whose stress is a callback evaluated every step."""
+    p = to_device(pts).contiguous()
+    n = p.shape[0]
+    st, caches = rollout(iso_growth_state(p, g), model, cfg, n_steps, advect)
+    F = st.F.double()
+    z3 = torch.zeros(n, 3, dtype=p.dtype, device=p.device)
+    z33 = torch.zeros(n, 3, 3, dtype=p.dtype, device=p.device)
+    if loss == "detF":
+        L = float(torch.linalg.det(F).sum())
+        Fb = (torch.linalg.det(F)[:, None, None] * torch.linalg.inv(F).transpose(1, 2)).to(p.dtype)
+        xb = z3
+    elif loss == "mse":
+        xo = to_device(x_obs, torch.float64, p.device).reshape(n, 3)
+        d = st.x.double() - xo
+        L = float((d * d).sum() / n)
+        xb, Fb = (2.0 * d / n).to(p.dtype), z33
+    else:
+        raise ValueError(loss)
+    bars = rollout_vjp(caches, xb, z3, z33, Fb, torch.zeros(n, 3, 3, dtype=torch.float64, device=p.device),
+                       advect)
+    return L, float(torch.diagonal(bars[4], dim1=-2, dim2=-1).sum())
 
 
 def lame_to_young(mu_bar: float, lam_bar: float, E: float, nu: float):
@@ -130,6 +159,8 @@ def dloss_dparams(pts, model, cfg, g, n_steps, advect, loss: str = "detF", x_obs
     no counterpart in the reference (its VJPs stop at F, Fg and C); they come
     from mpm_step_bwd_params.  Elastic models only (mu, lambda of the model)."""
     from .trajectory import Rollout
+    if is_external(model):
+        raise TypeError("material-parameter gradients need a built-in elastic model (mu, lambda)")
     p = to_device(pts).contiguous()
     n = p.shape[0]
     plan = get_plan([scene_spec(cfg, model, n)], p.dtype, p.device)

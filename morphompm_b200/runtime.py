@@ -163,6 +163,16 @@ class Plan:
         self.scenes = scenes
         self._c_scenes = arr
 
+    def set_external_stress(self, tau: Optional[torch.Tensor], tau_bar: Optional[torch.Tensor] = None):
+        """Caller-supplied Kirchhoff stress (n, 3, 3) for MPM_MODEL_EXTERNAL
+        scenes, and the buffer the reverse step writes its cotangent to."""
+        for a in (tau, tau_bar):
+            assert a is None or (a.is_contiguous() and a.dtype == self.dtype and a.numel() == 9 * self.n)
+        self._ext = (tau, tau_bar)
+        L.check(self.lib.mpm_plan_set_external_stress(
+            self.handle, C.c_void_p(tau.data_ptr() if tau is not None else 0),
+            C.c_void_p(tau_bar.data_ptr() if tau_bar is not None else 0)), "set_external_stress")
+
     def set_particle_mass(self, mass: Optional[torch.Tensor], vol0: Optional[torch.Tensor] = None):
         """Per-particle masses and reference volumes (None: the scenes' pmass / vol0)."""
         prep = lambda a: (a.to(device=self.device, dtype=self.dtype).contiguous() if a is not None else None)

@@ -18,6 +18,7 @@ from typing import List, Optional
 
 import torch
 
+from . import _lib as L
 from .runtime import Plan, SLAB_ROWS, ROW_F, ROW_X, slab_cotangents, slab_particles, stream_ptr
 
 
@@ -48,6 +49,9 @@ class Rollout:
     def __init__(self, plan: Plan, n_steps: int, advect: bool = True, ckpt_every: Optional[int] = None,
                  Fg: Optional[torch.Tensor] = None, loss: str = "detF", x_obs: Optional[torch.Tensor] = None,
                  material_grads: bool = False):
+        if any(int(sc.model) == L.MODEL_EXTERNAL for sc in plan.scenes):
+            raise TypeError("user-defined materials run through transfer.step / integrate.rollout "
+                            "(their stress is a callback evaluated every step)")
         self.plan = plan
         self.n_steps = int(n_steps)
         self.advect = bool(advect)

@@ -26,7 +26,7 @@ from typing import Optional
 import torch
 
 from . import _lib as L
-from .constitutive import model_fields
+from .constitutive import is_external, model_fields
 from .devarray import like_input, to_device
 from .runtime import Plan, SceneSpec, aos_cotangents, aos_particles
 from .state import ParticleState
@@ -64,7 +64,7 @@ def get_plan(specs, dtype, device, tuning=None) -> Plan:
 
 class StepCache:
     """Opaque record of one forward step (the reference's cache tuple)."""
-    __slots__ = ("plan", "tape", "x", "v", "C", "F", "Fg", "Cn", "advect", "ref", "t")
+    __slots__ = ("plan", "tape", "x", "v", "C", "F", "Fg", "Cn", "advect", "ref", "t", "model", "tau")
 
     def __init__(self, **kw):
         for k, v in kw.items():
@@ -91,10 +91,18 @@ def step(state: ParticleState, model, cfg, advect=True, t: int = 0):
     xn, vn = torch.empty_like(x), torch.empty_like(v)
     Cn, Fn, Fgn = torch.empty_like(Cm), torch.empty_like(F), torch.empty_like(Fg)
     tape = plan.new_tape()
+    tau = None
+    if is_external(model):
+        # a user-defined material: its batched stress, consumed by the kernels
+        tau = to_device(model.stress(F, Fg, Cm), dt, dev).reshape(n, 3, 3).contiguous()
+        plan.set_external_stress(tau, None)
     plan.step_fwd(aos_particles(x, v, Cm, F, Fg), aos_particles(xn, vn, Cn, Fn, Fgn), advect, t, tape)
+    if tau is not None:
+        plan.set_external_stress(None, None)
     _check(plan)
     new = ParticleState(*(like_input(a, ref) for a in (xn, vn, Cn, Fn, Fgn)))
-    cache = StepCache(plan=plan, tape=tape, x=x, v=v, C=Cm, F=F, Fg=Fg, Cn=Cn, advect=bool(advect), ref=ref, t=t)
+    cache = StepCache(plan=plan, tape=tape, x=x, v=v, C=Cm, F=F, Fg=Fg, Cn=Cn, advect=bool(advect), ref=ref, t=t,
+                      model=model, tau=tau)
     return new, cache
 
 
@@ -111,9 +119,22 @@ def step_vjp(cache: StepCache, xn_b, vn_b, Cn_b, Fn_b, Fgn_b, advect=True):
     xb, vb = torch.empty_like(xb_in), torch.empty_like(vb_in)
     Cb, Fb = torch.empty_like(Cb_in), torch.empty_like(Fb_in)
     Fgb = torch.empty_like(Fgb_in)
+    tau_bar = None
+    if cache.tau is not None:
+        tau_bar = torch.zeros_like(cache.tau)
+        plan.set_external_stress(cache.tau, tau_bar)
     plan.step_bwd(aos_particles(cache.x, cache.v, cache.C, cache.F, cache.Fg), cache.Cn.data_ptr(),
                   aos_cotangents(xb_in, vb_in, Cb_in, Fb_in, Fgb_in), aos_cotangents(xb, vb, Cb, Fb, Fgb),
                   None, advect, cache.t, cache.tape)
+    if tau_bar is not None:
+        plan.set_external_stress(None, None)
+        # the user material's own VJP of the stress it supplied
+        F_s, Fg_s, C_s = cache.model.stress_vjp(cache.F, cache.Fg, cache.C, tau_bar)
+        n = cache.F.shape[0]
+        Fb += to_device(F_s, dt, dev).reshape(n, 3, 3)
+        Fgb += to_device(Fg_s, torch.float64, dev).reshape(n, 3, 3)
+        if C_s is not None:
+            Cb += to_device(C_s, dt, dev).reshape(n, 3, 3)
     _check(plan)
     ref = cache.ref
     out = [like_input(a, ref) for a in (xb, vb, Cb, Fb)]

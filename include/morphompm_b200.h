@@ -226,6 +226,43 @@ int mpm_step_bwd_params(MpmPlan* plan, const MpmParticles* in, const void* out_C
                         double* growth_grad, double* material_grad, int32_t advect,
                         int32_t step_index, const void* tape, void* stream);
 
+/* ---- whole trajectories: checkpointed forward and adjoint ----
+ * Replace python/morphompm/integrate.py:15-28 (rollout, rollout_vjp), whose
+ * per-step caches are replaced here by checkpoint-every-k recomputation: the
+ * forward keeps the state at the start of every k-step segment, and the
+ * reverse recomputes one segment's states and tapes just before reversing it
+ * (ckpt_every = 0 or >= n_steps keeps every step and recomputes nothing).
+ * A state is a (24, n) slab of the plan's real type: rows x(3), v(3), C(9),
+ * F(9), row r of particle p at slab[r n + p]; cotangent slabs have the same
+ * layout.  Fg is NULL when every scene uses growth_mode 1, else a (9, n) slab
+ * of the real type (row c = 3 i + j).  Both calls are stream-ordered and
+ * capturable in one CUDA graph; neither allocates.  External-stress plans
+ * (MPM_MODEL_EXTERNAL) return MPM_ERR_UNSUPPORTED: their stress is a
+ * callback of every step (mpm_step_fwd / mpm_step_bwd). */
+
+/* Bytes of the rollout workspace for n_steps with checkpoints every ckpt_every
+ * (0 for n_steps == 0). */
+int mpm_rollout_workspace_bytes(const MpmPlan* plan, int32_t n_steps, int32_t ckpt_every, size_t* bytes);
+
+/* n_steps forward steps from state0 (not modified) into final_state, keeping
+ * in rollout_ws (256-byte aligned) what mpm_rollout_bwd needs.  Step t uses
+ * step_index t.  state0 and final_state must differ. */
+int mpm_rollout_fwd(MpmPlan* plan, const void* state0, const void* Fg, int32_t n_steps, int32_t ckpt_every,
+                    int32_t advect, void* rollout_ws, void* final_state, void* stream);
+
+/* Reverse sweep of the trajectory that the last mpm_rollout_fwd on
+ * rollout_ws ran (same Fg, n_steps, ckpt_every, advect; rollout_ws untouched
+ * in between).  final_bar (not modified) holds the cotangents of the final
+ * state, e.g. seeded by mpm_loss_detF / mpm_loss_mse into a zeroed slab;
+ * state0_bar (distinct from final_bar) receives those of state0.  Outputs,
+ * each overwritten and each optional: Fg_bar (9, n) double, d loss / d Fg
+ * summed over the steps (required when Fg is given and wanted); growth_grad
+ * (S) double, d loss / d A of growth_mode 1 scenes; material_grad (2 S)
+ * double, d loss / d (mu, lambda) per scene as in mpm_step_bwd_params. */
+int mpm_rollout_bwd(MpmPlan* plan, const void* Fg, const void* final_bar, int32_t n_steps, int32_t ckpt_every,
+                    int32_t advect, void* rollout_ws, void* state0_bar, double* Fg_bar, double* growth_grad,
+                    double* material_grad, void* stream);
+
 /* Batched constitutive seam: tau = model.stress(F, Fg, C) for n particles of one
  * scene's model.  Replaces constitutive.py:88-89,126-132. Arrays (n,3,3) C-contiguous. */
 int mpm_stress(const MpmScene* scene, int32_t real_bytes, int64_t n, const void* F,

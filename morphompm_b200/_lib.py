@@ -89,6 +89,9 @@ EXPORTS = {
     "mpm_stress": (i32, [C.POINTER(MpmScene), i32, i64, vp, vp, vp, vp, vp]),
     "mpm_stress_vjp": (i32, [C.POINTER(MpmScene), i32, i64, vp, vp, vp, vp, vp, vp, vp, vp]),
     "mpm_bin_keys": (i32, [C.POINTER(MpmScene), i32, i64, vp, vp, vp]),
+    "mpm_rollout_workspace_bytes": (i32, [vp, i32, i32, C.POINTER(C.c_size_t)]),
+    "mpm_rollout_fwd": (i32, [vp, vp, vp, i32, i32, i32, vp, vp, vp]),
+    "mpm_rollout_bwd": (i32, [vp, vp, vp, i32, i32, i32, vp, vp, vp, vp, vp, vp]),
     "mpm_loss_detF": (i32, [vp, vp, i64, i64, vp, vp, vp]),
     "mpm_loss_mse": (i32, [vp, vp, i64, i64, vp, vp, vp, vp]),
     "mpm_step_fwd_noalloc": (i32, [C.POINTER(MpmScene), i32, C.POINTER(MpmParticles), C.POINTER(MpmParticles),

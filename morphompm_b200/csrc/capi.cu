@@ -674,6 +674,196 @@ int mpm_step_bwd(MpmPlan* P, const MpmParticles* in, const void* out_C, const Mp
                                stream);
 }
 
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Whole trajectories (integrate.py:15-28 rollout / rollout_vjp, with the
+// per-step caches replaced by checkpoint-every-k recomputation).  The caller's
+// rollout workspace holds, 256-byte aligned and in this order:
+//   ckpt[n_seg]       state at the start of every segment   (recompute only)
+//   seg[k + 1]        the states of one segment
+//   scratch[2]        intermediate forward states           (recompute only)
+//   bars[2]           cotangent ping-pong of the reverse sweep
+//   tapes[k]          the tapes of one segment
+// Every slab is (24, n) in the plan's real type: rows x(3) v(3) C(9) F(9).
+// ---------------------------------------------------------------------------
+namespace {
+
+struct RolloutLayout {
+    int T = 0, k = 1, n_seg = 0;
+    bool recompute = false;
+    size_t slab = 0, tape = 0;
+    size_t o_ckpt = 0, o_seg = 0, o_scr = 0, o_bar = 0, o_tape = 0, total = 0;
+};
+
+bool rollout_layout(const MpmPlan* P, int n_steps, int ckpt_every, RolloutLayout& L) {
+    if (n_steps < 0 || ckpt_every < 0) return false;
+    L.T = n_steps;
+    L.k = ckpt_every > 0 ? std::min(ckpt_every, std::max(n_steps, 1)) : std::max(n_steps, 1);
+    L.n_seg = (n_steps + L.k - 1) / L.k;
+    L.recompute = L.k < n_steps;
+    L.slab = align_up((size_t)24 * (size_t)P->n * (size_t)P->real_bytes);
+    L.tape = align_up(P->tape_bytes);
+    Layout lay;
+    L.o_ckpt = lay.off;
+    if (L.recompute) lay.off += L.slab * L.n_seg;
+    L.o_seg = lay.off;
+    lay.off += L.slab * (L.k + 1);
+    L.o_scr = lay.off;
+    if (L.recompute) lay.off += L.slab * 2;
+    L.o_bar = lay.off;
+    lay.off += L.slab * 2;
+    L.o_tape = lay.off;
+    lay.off += L.tape * L.k;
+    L.total = n_steps == 0 ? 0 : lay.off;
+    return true;
+}
+
+MpmParticles slab_state(const MpmPlan* P, const void* slab, const void* Fg) {
+    const size_t row = (size_t)P->n * (size_t)P->real_bytes;
+    char* b = static_cast<char*>(const_cast<void*>(slab));
+    MpmParticles s{};
+    s.x = b;
+    s.v = b + 3 * row;
+    s.C = b + 6 * row;
+    s.F = b + 15 * row;
+    s.Fg = const_cast<void*>(Fg);
+    s.sp3 = s.sp9 = 1;
+    s.sc3 = s.sc9 = P->n;
+    return s;
+}
+
+MpmCotangents slab_cot(const MpmPlan* P, const void* slab, double* Fg_bar) {
+    MpmParticles v = slab_state(P, slab, nullptr);
+    MpmCotangents c{};
+    c.x = v.x;
+    c.v = v.v;
+    c.C = v.C;
+    c.F = v.F;
+    c.Fg = Fg_bar;
+    c.sp3 = c.sp9 = 1;
+    c.sc3 = c.sc9 = P->n;
+    return c;
+}
+
+int rollout_args(const MpmPlan* P, const void* Fg, const void* ws, const void* a, const void* b) {
+    if (!P || !P->ws || !a || !b || a == b) return MPM_ERR_ARG;
+    if (reinterpret_cast<uintptr_t>(ws) % ALIGN) return MPM_ERR_ARG;
+    if (P->any_external) return MPM_ERR_UNSUPPORTED;    // the stress is a per-step callback
+    for (const MpmScene& s : P->scenes)
+        if (s.growth_mode == 0 && !Fg) return MPM_ERR_ARG;
+    return MPM_OK;
+}
+
+inline int async_copy(void* dst, const void* src, size_t bytes, cudaStream_t st) {
+    return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, st) == cudaSuccess ? MPM_OK : MPM_ERR_CUDA;
+}
+
+// the chain flags of step t in a run of steps [t0, t1)
+inline int chain_flags(int t, int t0, int t1) {
+    return (t > t0 ? MPM_FWD_CHAINED : 0) | (t + 1 < t1 ? MPM_FWD_EMIT : 0);
+}
+
+}  // namespace
+
+extern "C" {
+
+int mpm_rollout_workspace_bytes(const MpmPlan* P, int32_t n_steps, int32_t ckpt_every, size_t* bytes) {
+    if (!P || !bytes) return MPM_ERR_ARG;
+    RolloutLayout L;
+    if (!rollout_layout(P, n_steps, ckpt_every, L)) return MPM_ERR_ARG;
+    *bytes = L.total;
+    return MPM_OK;
+}
+
+int mpm_rollout_fwd(MpmPlan* P, const void* state0, const void* Fg, int32_t n_steps, int32_t ckpt_every,
+                    int32_t advect, void* rollout_ws, void* final_state, void* stream) {
+    int rc = rollout_args(P, Fg, rollout_ws, state0, final_state);
+    if (rc) return rc;
+    RolloutLayout L;
+    if (!rollout_layout(P, n_steps, ckpt_every, L) || (L.total && !rollout_ws)) return MPM_ERR_ARG;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    char* w = static_cast<char*>(rollout_ws);
+    const size_t sb = (size_t)24 * (size_t)P->n * (size_t)P->real_bytes;
+    if (L.T == 0) return async_copy(final_state, state0, sb, st);
+    if (!L.recompute) {
+        // one segment: every state and tape is kept for the reverse sweep
+        if ((rc = async_copy(w + L.o_seg, state0, sb, st))) return rc;
+        for (int t = 0; t < L.T; ++t) {
+            MpmParticles a = slab_state(P, w + L.o_seg + L.slab * t, Fg);
+            MpmParticles b = slab_state(P, w + L.o_seg + L.slab * (t + 1), Fg);
+            rc = mpm_step_fwd_chain(P, &a, &b, advect, t, w + L.o_tape + L.tape * t, chain_flags(t, 0, L.T), st);
+            if (rc) return rc;
+        }
+        return async_copy(final_state, w + L.o_seg + L.slab * L.T, sb, st);
+    }
+    // checkpoints only; the intermediate states alternate between two scratch slabs
+    if ((rc = async_copy(w + L.o_ckpt, state0, sb, st))) return rc;
+    const char* cur = w + L.o_ckpt;
+    for (int t = 0; t < L.T; ++t) {
+        char* nxt;
+        if (t + 1 == L.T)
+            nxt = static_cast<char*>(final_state);
+        else if ((t + 1) % L.k == 0)
+            nxt = w + L.o_ckpt + L.slab * ((t + 1) / L.k);
+        else
+            nxt = w + L.o_scr + L.slab * ((cur == w + L.o_scr + L.slab * (t % 2)) ? (t + 1) % 2 : t % 2);
+        MpmParticles a = slab_state(P, cur, Fg), b = slab_state(P, nxt, Fg);
+        rc = mpm_step_fwd_chain(P, &a, &b, advect, t, nullptr, chain_flags(t, 0, L.T), st);
+        if (rc) return rc;
+        cur = nxt;
+    }
+    return MPM_OK;
+}
+
+int mpm_rollout_bwd(MpmPlan* P, const void* Fg, const void* final_bar, int32_t n_steps, int32_t ckpt_every,
+                    int32_t advect, void* rollout_ws, void* state0_bar, double* Fg_bar, double* growth_grad,
+                    double* material_grad, void* stream) {
+    int rc = rollout_args(P, Fg, rollout_ws, final_bar, state0_bar);
+    if (rc) return rc;
+    RolloutLayout L;
+    if (!rollout_layout(P, n_steps, ckpt_every, L) || (L.total && !rollout_ws)) return MPM_ERR_ARG;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const size_t S = P->scenes.size();
+    if ((Fg_bar && cudaMemsetAsync(Fg_bar, 0, (size_t)9 * P->n * sizeof(double), st) != cudaSuccess) ||
+        (growth_grad && cudaMemsetAsync(growth_grad, 0, S * sizeof(double), st) != cudaSuccess) ||
+        (material_grad && cudaMemsetAsync(material_grad, 0, 2 * S * sizeof(double), st) != cudaSuccess))
+        return MPM_ERR_CUDA;
+    char* w = static_cast<char*>(rollout_ws);
+    const size_t sb = (size_t)24 * (size_t)P->n * (size_t)P->real_bytes;
+    if (L.T == 0) return async_copy(state0_bar, final_bar, sb, st);
+    const void* cur = final_bar;
+    int flip = 0;
+    for (int seg = L.n_seg - 1; seg >= 0; --seg) {
+        const int t0 = seg * L.k, t1 = std::min(L.T, t0 + L.k);
+        if (L.recompute) {
+            // the segment's states and tapes again, from its checkpoint
+            if ((rc = async_copy(w + L.o_seg, w + L.o_ckpt + L.slab * seg, sb, st))) return rc;
+            for (int t = t0; t < t1; ++t) {
+                const int j = t - t0;
+                MpmParticles a = slab_state(P, w + L.o_seg + L.slab * j, Fg);
+                MpmParticles b = slab_state(P, w + L.o_seg + L.slab * (j + 1), Fg);
+                rc = mpm_step_fwd_chain(P, &a, &b, advect, t, w + L.o_tape + L.tape * j, chain_flags(t, t0, t1),
+                                        st);
+                if (rc) return rc;
+            }
+        }
+        for (int t = t1 - 1; t >= t0; --t) {
+            const int j = t - t0;
+            void* nxt = t == 0 ? state0_bar : static_cast<void*>(w + L.o_bar + L.slab * flip);
+            flip ^= 1;
+            MpmParticles a = slab_state(P, w + L.o_seg + L.slab * j, Fg);
+            const char* outC = w + L.o_seg + L.slab * (j + 1) + (size_t)6 * P->n * P->real_bytes;
+            MpmCotangents ob = slab_cot(P, cur, Fg_bar), ib = slab_cot(P, nxt, Fg_bar);
+            rc = mpm_step_bwd_params(P, &a, outC, &ob, &ib, growth_grad, material_grad, advect, t,
+                                     w + L.o_tape + L.tape * j, st);
+            if (rc) return rc;
+            cur = nxt;
+        }
+    }
+    return MPM_OK;
+}
+
 int mpm_stress(const MpmScene* scene, int32_t real_bytes, int64_t n, const void* F, const void* Fg, const void* C,
                void* tau, void* stream) {
     if (!scene || n < 0 || !F || !Fg || !tau || (real_bytes != 4 && real_bytes != 8)) return MPM_ERR_ARG;

@@ -35,6 +35,10 @@ def dtype_bytes(dtype) -> int:
     raise TypeError(f"unsupported dtype {dtype} (float32 or float64)")
 
 
+def _ptr(t: Optional[torch.Tensor]) -> int:
+    return t.data_ptr() if t is not None else 0
+
+
 def stream_ptr(stream=None) -> int:
     s = stream if stream is not None else torch.cuda.current_stream()
     return s.cuda_stream
@@ -256,6 +260,41 @@ class Plan:
                                              C.byref(ib), C.c_void_p(gg), C.c_void_p(material_grad.data_ptr()),
                                              int(bool(advect)), int(t), C.c_void_p(tape.ptr),
                                              C.c_void_p(stream_ptr(stream))), "mpm_step_bwd_params")
+
+    def rollout_workspace_bytes(self, n_steps: int, ckpt_every: int) -> int:
+        nb = C.c_size_t(0)
+        L.check(self.lib.mpm_rollout_workspace_bytes(self.handle, int(n_steps), int(ckpt_every), C.byref(nb)),
+                "mpm_rollout_workspace_bytes")
+        return nb.value
+
+    def rollout_fwd(self, state0: torch.Tensor, Fg: Optional[torch.Tensor], n_steps: int, ckpt_every: int,
+                    advect: bool, ws_ptr: int, final: torch.Tensor, stream=None):
+        """n_steps forward steps of (24, n) slab state0 into final, keeping the
+        checkpoints (or every step's state and tape) in the rollout workspace
+        (mpm_rollout_fwd)."""
+        for t in (state0, final):
+            assert t.dtype == self.dtype and t.shape == (SLAB_ROWS, self.n) and t.is_contiguous()
+        L.check(self.lib.mpm_rollout_fwd(self.handle, C.c_void_p(state0.data_ptr()), C.c_void_p(_ptr(Fg)),
+                                         int(n_steps), int(ckpt_every), int(bool(advect)), C.c_void_p(ws_ptr),
+                                         C.c_void_p(final.data_ptr()), C.c_void_p(stream_ptr(stream))),
+                "mpm_rollout_fwd")
+
+    def rollout_bwd(self, Fg: Optional[torch.Tensor], final_bar: torch.Tensor, n_steps: int, ckpt_every: int,
+                    advect: bool, ws_ptr: int, state0_bar: torch.Tensor, Fg_bar: Optional[torch.Tensor] = None,
+                    growth_grad: Optional[torch.Tensor] = None, material_grad: Optional[torch.Tensor] = None,
+                    stream=None):
+        """Reverse sweep of the last rollout_fwd on the workspace
+        (mpm_rollout_bwd); Fg_bar, growth_grad and material_grad are
+        overwritten float64 outputs."""
+        for t in (final_bar, state0_bar):
+            assert t.dtype == self.dtype and t.shape == (SLAB_ROWS, self.n) and t.is_contiguous()
+        for t in (Fg_bar, growth_grad, material_grad):
+            assert t is None or (t.dtype == torch.float64 and t.is_contiguous())
+        L.check(self.lib.mpm_rollout_bwd(self.handle, C.c_void_p(_ptr(Fg)), C.c_void_p(final_bar.data_ptr()),
+                                         int(n_steps), int(ckpt_every), int(bool(advect)), C.c_void_p(ws_ptr),
+                                         C.c_void_p(state0_bar.data_ptr()), C.c_void_p(_ptr(Fg_bar)),
+                                         C.c_void_p(_ptr(growth_grad)), C.c_void_p(_ptr(material_grad)),
+                                         C.c_void_p(stream_ptr(stream))), "mpm_rollout_bwd")
 
     def loss_detF(self, F_ptr: int, sp9: int, sc9: int, loss: torch.Tensor, F_bar_ptr: int = 0, stream=None):
         L.check(self.lib.mpm_loss_detF(self.handle, C.c_void_p(F_ptr), sp9, sc9, C.c_void_p(loss.data_ptr()),

@@ -1,7 +1,9 @@
 """Full-trajectory forward and adjoint on the device with checkpoint-every-k
 recomputation (the reference keeps every step's cache in RAM,
 python/morphompm/integrate.py:15-28; this engine keeps one state per segment
-and recomputes a segment's k states and tapes just before reversing it).
+and recomputes a segment's k states and tapes just before reversing it).  The
+step loops run natively behind the C ABI (mpm_rollout_fwd / mpm_rollout_bwd);
+this class owns their device buffers, the loss seed and graph capture.
 
 States are (24, n) slabs (runtime.py); cotangent slabs have the same layout.
 The Fg cotangent is a (9, n) float64 slab (explicit growth) or, for scenes in
@@ -19,7 +21,7 @@ from typing import List, Optional
 import torch
 
 from . import _lib as L
-from .runtime import Plan, SLAB_ROWS, ROW_F, ROW_X, slab_cotangents, slab_particles, stream_ptr
+from .runtime import Plan, SLAB_ROWS, ROW_F, ROW_X
 
 
 def sqrt_schedule(n_steps: int) -> int:
@@ -29,11 +31,13 @@ def sqrt_schedule(n_steps: int) -> int:
 
 def budget_schedule(n_steps: int, state_bytes: int, tape_bytes: int, budget: int) -> int:
     """Largest checkpoint interval k whose storage fits the byte budget:
-    ceil(N/k) checkpoints + (k+1) segment states + k tapes (k = N stores every
-    step and needs no recompute)."""
+    (k+1) segment states, 2 cotangent slabs, the final state, the loss seed
+    and the initial-state cotangents, k tapes, and with recompute (k < N)
+    ceil(N/k) checkpoints and 2 scratch states (k = N stores every step)."""
     best = 1
     for k in range(1, n_steps + 1):
-        need = ((n_steps + k - 1) // k + k + 1 + 5) * state_bytes + k * tape_bytes
+        extra = (n_steps + k - 1) // k + 2 if k < n_steps else 0
+        need = (extra + k + 1 + 5) * state_bytes + k * tape_bytes
         if need <= budget:
             best = k
     return best
@@ -63,14 +67,14 @@ class Rollout:
         self.loss_kind = loss
         self.x_obs = x_obs
         self.recompute = self.k < self.n_steps
-        # checkpoints (state at the start of every segment) + final state
-        self.ckpt = [torch.empty(SLAB_ROWS, n, dtype=dt, device=dev) for _ in range(self.n_seg)]
-        # per-segment states t0..t0+k and tapes t0..t0+k-1
-        self.seg_states = [torch.empty(SLAB_ROWS, n, dtype=dt, device=dev) for _ in range(self.k + 1)]
-        self.tapes = [plan.new_tape() for _ in range(self.k)]
+        # the checkpoints, segment states, tapes and cotangent ping-pong of the
+        # native trajectory engine (mpm_rollout_fwd / mpm_rollout_bwd)
+        self.ws_bytes = plan.rollout_workspace_bytes(self.n_steps, self.k)
+        self.ws = torch.empty(self.ws_bytes + 256, dtype=torch.uint8, device=dev)
+        self.ws_ptr = (self.ws.data_ptr() + 255) // 256 * 256
         self.final = torch.empty(SLAB_ROWS, n, dtype=dt, device=dev)
-        self.scratch = [torch.empty(SLAB_ROWS, n, dtype=dt, device=dev) for _ in range(2)]
-        self.bars = [torch.empty(SLAB_ROWS, n, dtype=dt, device=dev) for _ in range(2)]
+        self.seed_bar = torch.empty(SLAB_ROWS, n, dtype=dt, device=dev)     # loss seed: final-state cotangents
+        self.bar0_buf = torch.empty(SLAB_ROWS, n, dtype=dt, device=dev)     # initial-state cotangents
         self.Fg_bar = torch.zeros(9, n, dtype=torch.float64, device=dev) if Fg is not None else None
         S = len(plan.scenes)
         self.loss = torch.zeros(S, dtype=torch.float64, device=dev)
@@ -81,54 +85,24 @@ class Rollout:
         self.graph = None
 
     def memory_bytes(self) -> int:
-        es = self.plan.real_bytes
-        n = self.plan.n
-        slabs = len(self.ckpt) + len(self.seg_states) + 1 + 4
-        return slabs * SLAB_ROWS * n * es + len(self.tapes) * self.plan.tape_bytes
+        return self.ws_bytes + 3 * SLAB_ROWS * self.plan.n * self.plan.real_bytes
 
     # -- forward --------------------------------------------------------------
-    def _pp(self, slab):
-        return slab_particles(slab, self.Fg)
-
     def forward(self, slab0: torch.Tensor, stream=None) -> torch.Tensor:
-        """Run all steps from slab0; keeps the segment checkpoints.  When no
-        recompute is needed (k == n_steps), the tapes of the single segment are
-        recorded on the way."""
-        p = self.plan
-        self.ckpt[0].copy_(slab0)
-        if not self.recompute:
-            cur = self.seg_states[0]
-            cur.copy_(slab0)
-            for t in range(self.n_steps):
-                nxt = self.seg_states[t + 1]
-                p.step_fwd(self._pp(cur), self._pp(nxt), self.advect, t, self.tapes[t], stream,
-                           chained=t > 0, emit=t + 1 < self.n_steps)
-                cur = nxt
-            self.final.copy_(cur)
-            return self.final
-        cur = self.ckpt[0]
-        for t in range(self.n_steps):
-            if t + 1 == self.n_steps:
-                nxt = self.final
-            elif (t + 1) % self.k == 0:
-                nxt = self.ckpt[(t + 1) // self.k]
-            else:
-                nxt = self.scratch[t % 2] if cur is not self.scratch[t % 2] else self.scratch[(t + 1) % 2]
-            p.step_fwd(self._pp(cur), self._pp(nxt), self.advect, t, None, stream,
-                       chained=t > 0, emit=t + 1 < self.n_steps)
-            cur = nxt
+        """Run all steps from slab0 (mpm_rollout_fwd); keeps the segment
+        checkpoints, or, when no recompute is needed (k == n_steps), every
+        state and tape of the single segment."""
+        self.plan.rollout_fwd(slab0, self.Fg, self.n_steps, self.k, self.advect, self.ws_ptr, self.final, stream)
         return self.final
 
     # -- loss -----------------------------------------------------------------
     def seed(self, stream=None):
-        """Loss of the final state and its cotangent slab (bars[0])."""
+        """Loss of the final state and its cotangent slab."""
         p = self.plan
         n = p.n
         es = self.final.element_size()
-        b = self.bars[0]
+        b = self.seed_bar
         b.zero_()
-        if self.Fg_bar is not None:
-            self.Fg_bar.zero_()
         if self.loss_kind == "detF":
             p.loss_detF(self.final.data_ptr() + ROW_F * n * es, 1, n, self.loss, b.data_ptr() + ROW_F * n * es,
                         stream)
@@ -141,38 +115,14 @@ class Rollout:
 
     # -- adjoint --------------------------------------------------------------
     def backward(self, bar_T: Optional[torch.Tensor] = None, stream=None) -> torch.Tensor:
-        """Reverse sweep from cotangent slab bar_T (defaults to the loss seed in
-        bars[0]); returns the cotangent slab of the initial state."""
-        p = self.plan
-        if bar_T is not None and bar_T is not self.bars[0]:
-            self.bars[0].copy_(bar_T)
-        self.growth_grad.zero_()
-        if self.material_grad is not None:
-            self.material_grad.zero_()
-        cur_bar, nxt_bar = self.bars[0], self.bars[1]
-        for seg in range(self.n_seg - 1, -1, -1):
-            t0 = seg * self.k
-            t1 = min(self.n_steps, t0 + self.k)
-            if self.recompute:
-                st = self.seg_states
-                st[0].copy_(self.ckpt[seg])
-                for t in range(t0, t1):
-                    j = t - t0
-                    p.step_fwd(self._pp(st[j]), self._pp(st[j + 1]), self.advect, t, self.tapes[j], stream,
-                               chained=t > t0, emit=t + 1 < t1)
-            for t in range(t1 - 1, t0 - 1, -1):
-                j = t - t0
-                s_in = self.seg_states[j]
-                s_out = self.seg_states[j + 1]
-                n = p.n
-                es = s_out.element_size()
-                p.step_bwd(self._pp(s_in), s_out.data_ptr() + 6 * n * es,
-                           slab_cotangents(cur_bar, self.Fg_bar), slab_cotangents(nxt_bar, self.Fg_bar),
-                           self.growth_grad, self.advect, t, self.tapes[j], stream,
-                           material_grad=self.material_grad)
-                cur_bar, nxt_bar = nxt_bar, cur_bar
-        self.bar0 = cur_bar
-        return cur_bar
+        """Reverse sweep (mpm_rollout_bwd) from cotangent slab bar_T (defaults
+        to the loss seed); returns the cotangent slab of the initial state.
+        Fg_bar, growth_grad and material_grad receive this trajectory's sums."""
+        self.plan.rollout_bwd(self.Fg, bar_T if bar_T is not None else self.seed_bar, self.n_steps, self.k,
+                              self.advect, self.ws_ptr, self.bar0_buf, self.Fg_bar, self.growth_grad,
+                              self.material_grad, stream)
+        self.bar0 = self.bar0_buf
+        return self.bar0
 
     # -- graph capture ----------------------------------------------------------
     def run(self, slab0: torch.Tensor, stream=None):

@@ -111,3 +111,34 @@ def test_tape_grows_with_tile_cap():
         sizes.append(tb.value)
         lib.mpm_plan_destroy(h)
     assert sizes[1] < sizes[0]
+
+
+def test_rollout_workspace_layout():
+    """mpm_rollout_workspace_bytes (host only): k+1 segment states, 2 cotangent
+    slabs and k tapes; with recompute also ceil(N/k) checkpoints and 2 scratch
+    states.  Calls that would launch are refused on bad arguments first."""
+    lib = L.load()
+    arr = (L.MpmScene * 1)(_scene(1000, 0, (16, 16, 16)))
+    h = C.c_void_p()
+    assert lib.mpm_plan_create(arr, 1, 4, None, C.byref(h)) == 0
+    tb = C.c_size_t()
+    lib.mpm_plan_tape_bytes(h, C.byref(tb))
+    up = lambda b: (b + 255) // 256 * 256
+    slab, tape = up(24 * 1000 * 4), up(tb.value)
+
+    def ws(n, k):
+        nb = C.c_size_t(7)
+        assert lib.mpm_rollout_workspace_bytes(h, n, k, C.byref(nb)) == 0
+        return nb.value
+
+    assert ws(0, 0) == 0
+    assert ws(10, 0) == ws(10, 10) == ws(10, 99) == (11 + 2) * slab + 10 * tape
+    assert ws(10, 4) == (3 + 5 + 2 + 2) * slab + 4 * tape
+    assert ws(10, 1) == (10 + 2 + 2 + 2) * slab + 1 * tape
+    nb = C.c_size_t()
+    assert lib.mpm_rollout_workspace_bytes(h, -1, 0, C.byref(nb)) == L.MPM_ERR_ARG
+    assert lib.mpm_rollout_workspace_bytes(h, 5, -2, C.byref(nb)) == L.MPM_ERR_ARG
+    # unbound plan (no workspace): refused before any CUDA call
+    assert lib.mpm_rollout_fwd(h, 16, None, 3, 0, 1, None, 4096, None) == L.MPM_ERR_ARG
+    assert lib.mpm_rollout_bwd(h, None, 16, 3, 0, 1, None, 4096, None, None, None, None) == L.MPM_ERR_ARG
+    lib.mpm_plan_destroy(h)

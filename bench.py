@@ -457,7 +457,7 @@ def run_other(a):
         ob = Batch([c_true], c["steps"], dtype=torch.float64, ckpt_every=c["ckpt_every"])
         ob.load(host_slab([c_true], np.float64), non_blocking=False)
         ob.rollout.forward(ob.slab0)
-        x_obs = ob.rollout.final[0:3].t().cpu().numpy()
+        x_obs = ob.final_state()[0:3].t().cpu().numpy()
         c = dict(c, growth_A=c["g_eval"] - 1.0, ramp_steps=0)
         loss = "mse"
         del ob
@@ -481,7 +481,7 @@ def run_other(a):
                "trajectory_storage_gb": round(mem / 1e9, 2), "loss": float(b.loss[0]),
                "dloss_dg": float(b.dloss_dg[0]), "device_status": b.plan.status(),
                "fp64_hencky_fallbacks": b.plan.fp64_fallbacks()}
-        finals[key] = b.rollout.final.double().cpu().numpy()
+        finals[key] = b.final_state().double().cpu().numpy()
         if w == "config2":
             res["curvature"] = _curvature(finals[key])
             res["curvature_timoshenko"] = 1.5 * 0.2 / (8 * c["dx"])
@@ -525,8 +525,8 @@ def plain_leg(scn, a, value32, tuning32=None):
         b32.load(host_slab([s], np.float32), non_blocking=False)
         b32.run()
         torch.cuda.synchronize()
-        f64 = b64.rollout.final.cpu().numpy()
-        f32 = b32.rollout.final.double().cpu().numpy()
+        f64 = b64.final_state().cpu().numpy()
+        f32 = b32.final_state().double().cpu().numpy()
         errs["F"] = max(errs["F"], float(np.max(np.abs(f64[15:24] - f32[15:24]))))
         errs["x"] = max(errs["x"], float(np.max(np.abs(f64[0:3] - f32[0:3]))))
         g64, g32 = float(b64.dloss_dg[0]), float(b32.dloss_dg[0])

@@ -20,6 +20,7 @@ from typing import Optional
 
 import torch
 
+from .layout import cell_order_device
 from .runtime import ROW_X
 from .state import ParticleState
 
@@ -61,6 +62,9 @@ class _RolloutLoss(torch.autograd.Function):
         from .transfer import get_plan, scene_spec
         p = x0.detach().contiguous()
         n = p.shape[0]
+        order = cell_order_device(p, cfg.dx, cfg.grid_shape)     # memory layout only
+        if order is not None:
+            p = p[order].contiguous()
         plan = get_plan([scene_spec(cfg, model, n)], p.dtype, p.device)
         g = growth.detach()
         if g.dim() == 0:
@@ -68,14 +72,17 @@ class _RolloutLoss(torch.autograd.Function):
             for i in range(3):
                 Fg[4 * i] = g.to(p.dtype)
         else:
-            Fg = g.to(p.dtype).reshape(n, 9).t().contiguous()
+            gp = g.to(p.dtype).reshape(n, 9)
+            Fg = (gp if order is None else gp[order]).t().contiguous()
         xo = None
         if loss == "mse":
-            xo = x_obs.detach().to(device=p.device, dtype=p.dtype).reshape(n, 3).t().contiguous()
+            xo = x_obs.detach().to(device=p.device, dtype=p.dtype).reshape(n, 3)
+            xo = (xo if order is None else xo[order]).t().contiguous()
         ro = Rollout(plan, n_steps, advect=advect, ckpt_every=ckpt_every, Fg=Fg, loss=loss, x_obs=xo)
         ro.forward(_slab_from_points(p))
         ro.seed()
         ctx.ro = ro
+        ctx.order = order
         ctx.scalar_g = g.dim() == 0
         ctx.g_dtype = growth.dtype
         return ro.loss.sum().to(p.dtype)
@@ -87,8 +94,13 @@ class _RolloutLoss(torch.autograd.Function):
         n = ro.plan.n
         gx = (bar0[ROW_X:ROW_X + 3].t() * gL).contiguous()
         Fg_b = ro.Fg_bar.t().reshape(n, 3, 3) * gL.double()
+        if ctx.order is not None:
+            # back to the caller's particle order
+            gx = torch.empty_like(gx).index_copy_(0, ctx.order, gx)
+            Fg_b = torch.empty_like(Fg_b).index_copy_(0, ctx.order, Fg_b)
         gg = (Fg_b[:, 0, 0] + Fg_b[:, 1, 1] + Fg_b[:, 2, 2]).sum() if ctx.scalar_g else Fg_b
         ctx.ro = None
+        ctx.order = None
         return gx, gg.to(ctx.g_dtype), None, None, None, None, None, None, None
 
 

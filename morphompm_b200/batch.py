@@ -25,6 +25,7 @@ import torch
 from . import _lib as L
 from .runtime import Plan, SceneSpec, SLAB_ROWS, ROW_F, ROW_X
 from .trajectory import Rollout, budget_schedule, sqrt_schedule
+from .layout import batch_order
 
 MODEL_KIND = {"nh": L.MODEL_NEOHOOKEAN, "hencky": L.MODEL_HENCKY, "hb": L.MODEL_HERSCHEL_BULKLEY}
 
@@ -69,13 +70,16 @@ class Batch:
                  ckpt_every=None, tuning: Optional[dict] = None, loss: str = "detF",
                  x_obs: Optional[np.ndarray] = None, device=None, active_cap="auto",
                  memory_fraction: float = 0.75, slab_host: Optional[np.ndarray] = None,
-                 material_grads: bool = False):
+                 material_grads: bool = False, reorder: bool = True):
         """ckpt_every: int, None (store every step), "sqrt", or "auto" (largest
         interval that fits memory_fraction of the free device memory).
         active_cap: "auto" sizes the tapes' active-tile lists from a probe
         forward run of slab_host (1.25x its maximum), None keeps every tile.
         material_grads: also accumulate d loss / d (mu, lambda) per scene
-        (dloss_dmaterial, dloss_dE, dloss_dnu)."""
+        (dloss_dmaterial, dloss_dE, dloss_dnu).
+        reorder: store each scene's particles in the cell order of their
+        initial positions (layout.py); inputs and the state accessors keep the
+        caller's particle order."""
         self.scenes = [dict(s) for s in scenes]   # set_params edits these copies
         self.n_steps = n_steps
         self.dtype = dtype
@@ -83,12 +87,18 @@ class Batch:
         self.n = sum(sp.n for sp in self.specs)
         npd = np.float32 if dtype == torch.float32 else np.float64
         tuning = dict(tuning or {})
+        offsets = np.concatenate([[0], np.cumsum([sp.n for sp in self.specs])]).astype(np.int64)
+        self.order = batch_order(scenes, offsets) if reorder else None     # slot -> input particle
         phi = host_phi(scenes, npd)
+        if phi is not None and self.order is not None:
+            phi = np.ascontiguousarray(phi[self.order])
         if active_cap == "auto":
             probe = Plan(self.specs, dtype=dtype, tuning=tuning, device=device)
             self._set_phi(probe, phi)
-            tuning["active_tile_cap"] = self._probe_active(probe, slab_host if slab_host is not None
-                                                           else host_slab(scenes, npd), advect)
+            sh = slab_host if slab_host is not None else host_slab(scenes, npd)
+            if self.order is not None:
+                sh = np.ascontiguousarray(np.asarray(sh)[:, self.order])
+            tuning["active_tile_cap"] = self._probe_active(probe, sh, advect)
             del probe
         elif active_cap:
             tuning["active_tile_cap"] = int(active_cap)
@@ -103,10 +113,17 @@ class Batch:
         self.ckpt_every = ckpt_every or n_steps
         xo = None
         if loss == "mse":
-            xo = torch.as_tensor(np.ascontiguousarray(x_obs.T.astype(npd))).to(self.plan.device)
+            xob = x_obs if self.order is None else x_obs[self.order]
+            xo = torch.as_tensor(np.ascontiguousarray(xob.T.astype(npd))).to(self.plan.device)
         self.rollout = Rollout(self.plan, n_steps, advect=advect, ckpt_every=self.ckpt_every, Fg=None, loss=loss,
                                x_obs=xo, material_grads=material_grads)
         self.slab0 = torch.empty(SLAB_ROWS, self.n, dtype=dtype, device=self.plan.device)
+        self.order_dev = self.inverse_dev = self._stage = None
+        if self.order is not None:
+            dev = self.plan.device
+            self.order_dev = torch.as_tensor(self.order).to(dev)
+            self.inverse_dev = torch.as_tensor(np.argsort(self.order)).to(dev)
+            self._stage = torch.empty(SLAB_ROWS, self.n, dtype=dtype, device=dev)
         self.graph = None
 
     @staticmethod
@@ -138,7 +155,26 @@ class Batch:
     def load(self, slab_host: np.ndarray, non_blocking=True):
         """Copy a (24, n) host slab (pinned for async) into the device input."""
         src = torch.from_numpy(slab_host) if isinstance(slab_host, np.ndarray) else slab_host
-        self.slab0.copy_(src, non_blocking=non_blocking)
+        if self.order is None:
+            self.slab0.copy_(src, non_blocking=non_blocking)
+        else:
+            # the caller's particle order -> the batch's cell order, on the device
+            self._stage.copy_(src, non_blocking=non_blocking)
+            torch.index_select(self._stage, 1, self.order_dev, out=self.slab0)
+
+    def _to_input_order(self, slab: torch.Tensor) -> torch.Tensor:
+        if self.order is None:
+            return slab
+        return torch.index_select(slab, 1, self.inverse_dev)
+
+    def final_state(self) -> torch.Tensor:
+        """(24, n) final state of the last trajectory, in the caller's particle order."""
+        return self._to_input_order(self.rollout.final)
+
+    def initial_cotangents(self) -> torch.Tensor:
+        """(24, n) d loss / d (initial state) of the last trajectory, in the
+        caller's particle order."""
+        return self._to_input_order(self.rollout.bar0)
 
     def run(self):
         return self.rollout.run(self.slab0)

@@ -8,7 +8,7 @@ signatures (python/morphompm/integrate.py:15-52):
 
 ``rollout``/``rollout_vjp`` keep one cache per step like the reference (device
 memory O(n_steps)).  ``dloss_dg`` runs the device trajectory engine
-(trajectory.Rollout) instead, with optional checkpoint-every-k recomputation
+(trajectory.Rollout) instead, on the particles in cell order (layout.py), with optional checkpoint-every-k recomputation
 (``ckpt_every``) and an optional mean-squared final-position loss
 (``loss="mse"``, ``x_obs``); with the defaults it returns what the reference
 returns.
@@ -24,6 +24,7 @@ from .devarray import like_input, to_device
 from .runtime import SLAB_ROWS, ROW_C, ROW_F, ROW_V, ROW_X
 from .state import ParticleState
 from .constitutive import is_external
+from .layout import cell_order_device
 from .transfer import get_plan, scene_spec, step, step_vjp
 
 
@@ -100,6 +101,11 @@ def dloss_dg(pts, model, cfg, g, n_steps, advect, loss: str = "detF", x_obs=None
         return _dloss_dg_steps(pts, model, cfg, g, n_steps, advect, loss, x_obs)
     p = to_device(pts).contiguous()
     n = p.shape[0]
+    if n == 0:
+        return 0.0, 0.0     # no particles: sum det F over none
+    order = cell_order_device(p, cfg.dx, cfg.grid_shape)     # memory layout only
+    if order is not None:
+        p = p[order].contiguous()
     plan = get_plan([scene_spec(cfg, model, n)], p.dtype, p.device)
     Fg = torch.zeros(9, n, dtype=p.dtype, device=p.device)
     for i in range(3):
@@ -107,6 +113,8 @@ def dloss_dg(pts, model, cfg, g, n_steps, advect, loss: str = "detF", x_obs=None
     xo = None
     if loss == "mse":
         xo_t = to_device(x_obs, p.dtype, p.device).reshape(n, 3)
+        if order is not None:
+            xo_t = xo_t[order]
         xo = xo_t.t().contiguous()
     ro = Rollout(plan, n_steps, advect=advect, ckpt_every=ckpt_every, Fg=Fg, loss=loss, x_obs=xo)
     ro.run(_slab_from_points(p))
@@ -121,6 +129,8 @@ def _dloss_dg_steps(pts, model, cfg, g, n_steps, advect, loss, x_obs):
     whose stress is a callback evaluated every step."""
     p = to_device(pts).contiguous()
     n = p.shape[0]
+    if n == 0:
+        return 0.0, 0.0
     st, caches = rollout(iso_growth_state(p, g), model, cfg, n_steps, advect)
     F = st.F.double()
     z3 = torch.zeros(n, 3, dtype=p.dtype, device=p.device)
@@ -163,13 +173,21 @@ def dloss_dparams(pts, model, cfg, g, n_steps, advect, loss: str = "detF", x_obs
         raise TypeError("material-parameter gradients need a built-in elastic model (mu, lambda)")
     p = to_device(pts).contiguous()
     n = p.shape[0]
+    if n == 0:
+        return 0.0, {"g": 0.0, "mu": 0.0, "lam": 0.0, "E": 0.0, "nu": 0.0}
+    order = cell_order_device(p, cfg.dx, cfg.grid_shape)     # memory layout only
+    if order is not None:
+        p = p[order].contiguous()
     plan = get_plan([scene_spec(cfg, model, n)], p.dtype, p.device)
     Fg = torch.zeros(9, n, dtype=p.dtype, device=p.device)
     for i in range(3):
         Fg[4 * i] = g
     xo = None
     if loss == "mse":
-        xo = to_device(x_obs, p.dtype, p.device).reshape(n, 3).t().contiguous()
+        xo_t = to_device(x_obs, p.dtype, p.device).reshape(n, 3)
+        if order is not None:
+            xo_t = xo_t[order]
+        xo = xo_t.t().contiguous()
     ro = Rollout(plan, n_steps, advect=advect, ckpt_every=ckpt_every, Fg=Fg, loss=loss, x_obs=xo,
                  material_grads=True)
     ro.run(_slab_from_points(p))

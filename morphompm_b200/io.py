@@ -122,12 +122,13 @@ def _save_vtk(st, path):
 # -- batches ------------------------------------------------------------------
 def save_batch(batch, path_pattern, slab=None):
     """Write each scene of a ``batch.Batch`` to path_pattern.format(s=index),
-    from a (24, n) slab (default: the final state of the last trajectory).
+    from a (24, n) slab in the scenes' particle order (default: the final
+    state of the last trajectory).
     The growth tensor is the scene's growth law at the end of the trajectory,
     g I with g = 1 + A ramp(n_steps - 1) phi."""
     from .runtime import ROW_C, ROW_F, ROW_V, ROW_X
     from .batch import host_phi
-    s_all = _host(batch.rollout.final if slab is None else slab).astype(np.float64)
+    s_all = _host(batch.final_state() if slab is None else slab).astype(np.float64)
     phi = host_phi(batch.scenes, np.float64)
     paths = []
     for s, (p0, p1) in enumerate(zip(batch.plan.offsets[:-1], batch.plan.offsets[1:])):

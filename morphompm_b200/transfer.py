@@ -87,6 +87,11 @@ def step(state: ParticleState, model, cfg, advect=True, t: int = 0):
     F = to_device(state.F, dt, dev).contiguous()
     Fg = to_device(state.Fg, dt, dev).contiguous()
     n = x.shape[0]
+    if n == 0:
+        # no particles: an empty grid, nothing moves (transfer.py:33-79 loops over none)
+        new = ParticleState(*(like_input(a.clone(), ref) for a in (x, v, Cm, F, Fg)))
+        return new, StepCache(plan=None, tape=None, x=x, v=v, C=Cm, F=F, Fg=Fg, Cn=Cm, advect=bool(advect),
+                              ref=ref, t=t, model=model, tau=None)
     plan = get_plan([scene_spec(cfg, model, n)], dt, dev)
     xn, vn = torch.empty_like(x), torch.empty_like(v)
     Cn, Fn, Fgn = torch.empty_like(Cm), torch.empty_like(F), torch.empty_like(Fg)
@@ -111,6 +116,13 @@ def step_vjp(cache: StepCache, xn_b, vn_b, Cn_b, Fn_b, Fgn_b, advect=True):
     a frozen input and x_b is returned as 0."""
     plan = cache.plan
     dt, dev = cache.x.dtype, cache.x.device
+    if plan is None:
+        # the step of an empty state: empty cotangents
+        ref = cache.ref
+        out = [like_input(torch.zeros_like(a), ref) for a in (cache.x, cache.v, cache.C, cache.F)]
+        Fgb = torch.zeros(cache.Fg.shape, dtype=torch.float64, device=dev)
+        out.append(like_input(Fgb, ref) if not isinstance(ref, torch.Tensor) else Fgb)
+        return tuple(out)
     xb_in = to_device(xn_b, dt, dev).contiguous()
     vb_in = to_device(vn_b, dt, dev).contiguous()
     Cb_in = to_device(Cn_b, dt, dev).contiguous()

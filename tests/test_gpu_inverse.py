@@ -71,7 +71,7 @@ def test_fit_batched_recovers_modulus():
     truth = _batch(sc, 30)
     truth.set_params(E=E_true)
     truth.rollout.forward(truth.slab0)
-    x_obs = truth.rollout.final[0:3].t().cpu().numpy().copy()
+    x_obs = truth.final_state()[0:3].t().cpu().numpy().copy()
     fit = _batch(sc, 30, loss="mse", x_obs=x_obs, material_grads=True)
     res = diff.fit_batched(fit, params=("E",), iters=60, lr=0.05, E0=E_true * np.array([1.5, 0.7]))
     assert (res["loss"][-1] < 1e-3 * res["loss"][0]).all(), res["loss"][[0, -1]]

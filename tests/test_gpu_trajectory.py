@@ -141,7 +141,7 @@ def test_config1_free_swell_fp64_matches_oracle_1e10():
         b = Batch([c], c["steps"], dtype=dt, ckpt_every=10)
         b.load(host_slab([c], np.float64 if dt == torch.float64 else np.float32), non_blocking=False)
         b.rollout.forward(b.slab0)
-        fin = b.rollout.final.double().cpu().numpy()
+        fin = b.final_state().double().cpu().numpy()
         F = fin[15:24].T.reshape(-1, 3, 3)
         x = fin[0:3].T
         res[dt] = (np.max(np.abs(F - st.F)), np.max(np.abs(x - st.x)))
@@ -187,7 +187,7 @@ def test_save_batch_writes_each_scene(tmp_path):
     b.load(host_slab(sc, np.float32), non_blocking=False)
     b.rollout.forward(b.slab0)
     paths = mio.save_batch(b, str(tmp_path / "scene{s}.npz"))
-    fin = b.rollout.final.double().cpu().numpy()
+    fin = b.final_state().double().cpu().numpy()
     p0 = 0
     for s, path in enumerate(paths):
         st = mio.load_state(path)

@@ -311,6 +311,15 @@ int mpm_loss_mse(MpmPlan* plan, const void* x, int64_t sp3, int64_t sc3, const v
 int mpm_step_fwd_noalloc(const MpmScene* scene, int32_t real_bytes, const MpmParticles* in, MpmParticles* out,
                          int32_t advect, int32_t step_index, int32_t* status, void* stream);
 
+/* Bounds-checked build (the same sources compiled with MPM_CHECK_BOUNDS into
+ * libmorphompm_b200_checked.so): every index the kernels compute into node,
+ * cell-sum, segment, tile and sort arrays is checked; an index out of range is
+ * counted and its access skipped.  Returns the number counted since the last
+ * call with the site id and index of the first, and resets the count
+ * (stream-ordered, synchronizes the stream).  The release library returns
+ * MPM_ERR_UNSUPPORTED. */
+int mpm_check_violations(int64_t* count, int32_t* first_site, int64_t* first_index, void* stream);
+
 int mpm_version(void);
 
 #ifdef __cplusplus

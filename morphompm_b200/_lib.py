@@ -9,7 +9,10 @@ from __future__ import annotations
 import ctypes as C
 import os
 
-from .build import LIB, build, up_to_date
+from .build import LIB, LIB_CHECKED, build, up_to_date
+
+# MORPHOMPM_CHECKED=1: the bounds-checked build of the same sources
+CHECKED = os.environ.get("MORPHOMPM_CHECKED", "0") == "1"
 
 MPM_OK = 0
 MPM_ERR_ARG = 1
@@ -96,13 +99,14 @@ EXPORTS = {
     "mpm_loss_mse": (i32, [vp, vp, i64, i64, vp, vp, vp, vp]),
     "mpm_step_fwd_noalloc": (i32, [C.POINTER(MpmScene), i32, C.POINTER(MpmParticles), C.POINTER(MpmParticles),
                                    i32, i32, C.POINTER(i32), vp]),
+    "mpm_check_violations": (i32, [C.POINTER(i64), C.POINTER(i32), C.POINTER(i64), vp]),
 }
 
 _lib = None
 
 
 def lib_path() -> str:
-    return LIB
+    return LIB_CHECKED if CHECKED else LIB
 
 
 def load(build_if_missing: bool = True):
@@ -110,11 +114,12 @@ def load(build_if_missing: bool = True):
     global _lib
     if _lib is not None:
         return _lib
-    if not os.path.exists(LIB) or (build_if_missing and not up_to_date()):
+    path = lib_path()
+    if not os.path.exists(path) or (build_if_missing and not up_to_date(CHECKED)):
         if not build_if_missing:
-            raise RuntimeError(f"morphompm_b200 CUDA library not built: {LIB}")
-        build()
-    lib = C.CDLL(LIB)
+            raise RuntimeError(f"morphompm_b200 CUDA library not built: {path}")
+        build(checked=CHECKED)
+    lib = C.CDLL(path)
     for name, (res, args) in EXPORTS.items():
         fn = getattr(lib, name)
         fn.restype = res

@@ -2,6 +2,7 @@
 // workspace/tape layout, and the launch sequences of one forward and one
 // reverse growth step.  No device memory is allocated here.
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <algorithm>
 #include <atomic>
@@ -103,6 +104,9 @@ Ctx make_ctx(MpmPlan* P) {
     c.dense_b = P->ws + P->o_dense_b;
     c.n = P->n;
     c.n_tiles = P->n_tiles;
+    c.n_keys = P->n_keys;
+    c.n_nodes = P->n_nodes;
+    c.grid_nodes = (long long)P->active_cap * P->TN;
     c.n_scenes = (int)P->scenes.size();
     c.tile_xy = P->tune.tile_xy;
     c.tile_z = P->tune.tile_z;
@@ -136,13 +140,19 @@ void record_event(cudaEvent_t e, cudaStream_t st) {
                                                                         : cudaEventRecordDefault);
 }
 
-// Brackets one launch site: counts its kernels and, when profiling this kind,
-// records start/stop events around it.
+// NVTX range names of the kernel kinds (MPM_K_*), for profilers' filters
+const char* const KIND_NAME[MPM_K_COUNT] = {"mpm.bin", "mpm.sort", "mpm.mark", "mpm.compact",
+                                            "mpm.prepass", "mpm.p2g", "mpm.g2p", "mpm.bwd_payload",
+                                            "mpm.bwd_p2g", "mpm.bwd_particle", "mpm.reduce"};
+
+// Brackets one launch site: an NVTX range named for its kind, the launch
+// count, and, when profiling this kind, start/stop events around it.
 struct Site {
     MpmPlan* P;
     cudaStream_t st;
     bool on;
     Site(MpmPlan* p, int kind, int kernels, cudaStream_t s) : P(p), st(s) {
+        nvtxRangePushA(KIND_NAME[kind]);
         P->launches += kernels;
         on = ((P->prof_mask >> kind) & 1u) && P->prof_n < P->prof_max;
         if (on) {
@@ -155,6 +165,7 @@ struct Site {
             record_event(P->ev1[P->prof_n], st);
             ++P->prof_n;
         }
+        nvtxRangePop();
     }
 };
 
@@ -370,6 +381,31 @@ bool scene_ok(const MpmScene& s) {
 extern "C" {
 
 int mpm_version(void) { return 1; }
+
+int mpm_check_violations(int64_t* count, int32_t* first_site, int64_t* first_index, void* stream) {
+    if (!count) return MPM_ERR_ARG;
+    *count = 0;
+#ifdef MPM_CHECK_BOUNDS
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    unsigned long long c = 0;
+    long long first[2] = {0, -1};
+    const unsigned long long zero = 0;
+    if (cudaMemcpyFromSymbolAsync(&c, g_oob_count, sizeof(c), 0, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaMemcpyFromSymbolAsync(first, g_oob_first, sizeof(first), 0, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaMemcpyToSymbolAsync(g_oob_count, &zero, sizeof(zero), 0, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
+        return MPM_ERR_CUDA;
+    *count = (int64_t)c;
+    if (first_site) *first_site = c ? (int32_t)first[0] : 0;
+    if (first_index) *first_index = c ? (int64_t)first[1] : -1;
+    return MPM_OK;
+#else
+    (void)stream;
+    if (first_site) *first_site = 0;
+    if (first_index) *first_index = -1;
+    return MPM_ERR_UNSUPPORTED;
+#endif
+}
 
 int mpm_plan_create(const MpmScene* scenes, int32_t n_scenes, int32_t real_bytes, const MpmTuning* tuning,
                     MpmPlan** out) {

@@ -12,6 +12,33 @@
 
 namespace mpm {
 
+// ---------------------------------------------------------------------------
+// Bounds-checked build (compiled with -DMPM_CHECK_BOUNDS): every index the
+// kernels compute into the node, sum, segment, tile and sort arrays is checked
+// against the array's size before the access.  An index out of range is
+// counted, the first one is recorded (site id, index), and the access is
+// skipped, so a wrong index shows up as a count instead of a memory fault.
+// The release build compiles the checks away (MPM_INB is the constant true).
+// Site ids: 1 tile flag, 2 cell mark, 3 segment table write, 4 cell-sum
+// store, 5 cell-sum load, 6 cell mark read, 7 dense node record, 8 tape grid
+// record, 9 sort permutation value, 10 sort scatter, 11 segment range read.
+// ---------------------------------------------------------------------------
+#ifdef MPM_CHECK_BOUNDS
+__device__ unsigned long long g_oob_count;
+__device__ long long g_oob_first[2];
+__device__ __forceinline__ bool in_bounds(long long i, long long n, int site) {
+    if (i >= 0 && i < n) return true;
+    if (atomicAdd(&g_oob_count, 1ull) == 0ull) {
+        g_oob_first[0] = site;
+        g_oob_first[1] = i;
+    }
+    return false;
+}
+#define MPM_INB(i, n, site) ::mpm::in_bounds((long long)(i), (long long)(n), (site))
+#else
+#define MPM_INB(i, n, site) true
+#endif
+
 // Node tiles are tile_xy x tile_xy x tile_z nodes (z fastest inside a tile).
 
 // Per-scene data derived on the host from MpmScene.
@@ -46,6 +73,9 @@ struct Ctx {
     void* dense_b;               // dense node scratch, reverse record (gm_b, gmom_b[3]) per node
     long long n;
     long long n_tiles;
+    long long n_keys;            // padded cells of all scenes (cell_seg entries)
+    long long n_nodes;           // nodes of all scenes (dense_f / dense_b records)
+    long long grid_nodes;        // node records of a tape's grid (active_cap x nodes per tile)
     int n_scenes;
     int tile_xy;
     int tile_z;

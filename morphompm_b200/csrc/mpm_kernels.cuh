@@ -201,7 +201,10 @@ __device__ __forceinline__ void flag_tiles(const Ctx& ctx, long long s, unsigned
     for (int a = tlo[0]; a <= thi[0]; ++a)
         for (int b = tlo[1]; b <= thi[1]; ++b)
             for (int e = tlo[2]; e <= thi[2]; ++e)
-                ctx.tile_flag[ax.tile_begin + ((long long)a * ax.ntile[1] + b) * ax.ntile[2] + e] = 1;
+            {
+                const long long ti = ax.tile_begin + ((long long)a * ax.ntile[1] + b) * ax.ntile[2] + e;
+                if (MPM_INB(ti, ctx.n_tiles, 1)) ctx.tile_flag[ti] = 1;
+            }
 }
 
 // Slots of a block are visited warp-striped (slot = block base + round*256 +
@@ -271,8 +274,12 @@ scan_counts_kernel(unsigned* __restrict__ cnt, int nblk, int* __restrict__ total
 __global__ void __launch_bounds__(256)
 remark_cells_kernel(Ctx ctx, const unsigned* __restrict__ skeys) {
     const int nseg = *ctx.n_seg;
-    for (int id = blockIdx.x * blockDim.x + threadIdx.x; id < nseg; id += gridDim.x * blockDim.x)
-        ctx.cell_seg[skeys[ctx.seg_first[id]]] = id + 1;
+    for (int id = blockIdx.x * blockDim.x + threadIdx.x; id < nseg; id += gridDim.x * blockDim.x) {
+        const int f = ctx.seg_first[id];
+        if (!MPM_INB(f, ctx.n, 11)) continue;
+        const unsigned k = skeys[f];
+        if (MPM_INB(k, ctx.n_keys, 2)) ctx.cell_seg[k] = id + 1;
+    }
 }
 
 // Active-tile list: the tiles flagged by the segment count pass, in tile
@@ -358,15 +365,16 @@ seg_write_kernel(Ctx ctx, const unsigned* __restrict__ skeys) {
         before += __popc(ball & lt);
         // starts up to and including s, minus one: the segment id of slot s
         const unsigned id = before + (start ? 1u : 0u);
-        if (start) {
+        if (start && MPM_INB(id - 1, ctx.n, 3)) {
             ctx.seg_first[id - 1] = (int)s;
-            ctx.cell_seg[k] = (int)id;
+            if (MPM_INB(k, ctx.n_keys, 2)) ctx.cell_seg[k] = (int)id;
         }
         if (valid && id > 0) {
             const bool last = s == ctx.n - 1 || skeys[s + 1] != k;
             if (last) {
                 const SceneAux& ax = ctx.aux[ctx.scene_of[s]];
-                if ((long long)k - ax.cell_begin < ax.ncells) ctx.seg_last[id - 1] = (int)(s + 1);
+                if ((long long)k - ax.cell_begin < ax.ncells && MPM_INB(id - 1, ctx.n, 3))
+                    ctx.seg_last[id - 1] = (int)(s + 1);
             }
         }
         run += round;
@@ -507,7 +515,7 @@ __device__ __forceinline__ void store_acc(R* __restrict__ S, long long cap, int 
 #pragma unroll
             for (int oz = 0; oz < 3; ++oz) {
                 const int o = 9 * (ox0 + a) + 3 * oy + oz;
-                store_sum(S, (long long)o * cap + id, acc[a][oy][oz]);
+                if (MPM_INB((long long)o * cap + id, 27 * cap, 4)) store_sum(S, (long long)o * cap + id, acc[a][oy][oz]);
             }
 }
 
@@ -524,10 +532,12 @@ cell_sums_kernel(Ctx ctx, const unsigned* __restrict__ perm, const R* __restrict
              g += (long long)gridDim.x * blockDim.x) {
             const int id = (int)(g / 3), ox0 = (int)(g % 3);
             const int first = ctx.seg_first[id], last = ctx.seg_last[id];
+            if (!(MPM_INB(first, ctx.n + 1, 11) && MPM_INB(last, ctx.n + 1, 11))) continue;
             R acc[1][3][3][4];
             zero_acc<R, 1>(acc);
             for (int q = first; q < last; ++q) {
                 R r[PAYLOAD];
+                if (!MPM_INB(perm[q], ctx.n, 9)) continue;
                 load_record(payload, perm[q], r);
                 accumulate_record<R, MODE, 1>(r, ox0, acc);
             }
@@ -536,12 +546,14 @@ cell_sums_kernel(Ctx ctx, const unsigned* __restrict__ perm, const R* __restrict
     } else {
         for (int id = blockIdx.x * blockDim.x + threadIdx.x; id < nseg; id += gridDim.x * blockDim.x) {
             const int first = ctx.seg_first[id], last = ctx.seg_last[id];
+            if (!(MPM_INB(first, ctx.n + 1, 11) && MPM_INB(last, ctx.n + 1, 11))) continue;
 #pragma unroll 1
             for (int ox0 = 0; ox0 < 3; ox0 += OXB) {
                 R acc[OXB][3][3][4];
                 zero_acc<R, OXB>(acc);
                 for (int q = first; q < last; ++q) {
                     R r[PAYLOAD];
+                    if (!MPM_INB(perm[q], ctx.n, 9)) continue;
                     load_record(payload, perm[q], r);
                     accumulate_record<R, MODE, OXB>(r, ox0, acc);
                 }
@@ -563,6 +575,7 @@ __device__ __forceinline__ void adj_cell(const Ctx& ctx, const unsigned* __restr
                                          const MpmCotangents& ob, R* __restrict__ S, long long cap, int advect,
                                          int id, int ox_lo, int ox_hi) {
     const int first = ctx.seg_first[id], last = ctx.seg_last[id];
+    if (!(MPM_INB(first, ctx.n, 11) && MPM_INB(last, ctx.n + 1, 11))) return;
     const MpmScene& sc = ctx.scenes[ctx.scene_of[first]];
     const R dx = (R)sc.dx, dt = (R)sc.dt, inv_dx = (R)(1.0 / sc.dx);
     const R kdx = R(4) * inv_dx * inv_dx * dx;
@@ -579,6 +592,7 @@ __device__ __forceinline__ void adj_cell(const Ctx& ctx, const unsigned* __restr
                     for (int h = 0; h < 3; ++h) acc[a][b][c][h] = R(0);
         for (int q = first; q < last; ++q) {
             const long long p = perm[q];
+            if (!MPM_INB(p, ctx.n, 9)) continue;
             R x[3], nv[3], B[9];
             ld3<R>(in.x, p, in.sp3, in.sc3, x);
             {
@@ -634,7 +648,7 @@ __device__ __forceinline__ void adj_cell(const Ctx& ctx, const unsigned* __restr
                 for (int oz = 0; oz < 3; ++oz) {
                     const int o = 9 * (ox0 + a) + 3 * oy + oz;
                     const R v4[4] = {acc[a][oy][oz][0], acc[a][oy][oz][1], acc[a][oy][oz][2], R(0)};
-                    store_sum(S, (long long)o * cap + id, v4);
+                    if (MPM_INB((long long)o * cap + id, 27 * cap, 4)) store_sum(S, (long long)o * cap + id, v4);
                 }
     }
 }
@@ -714,14 +728,17 @@ node_sums_kernel(Ctx ctx, const R* __restrict__ S, long long cap, const int* __r
                 for (int oy = 0; oy < 3; ++oy)
 #pragma unroll
                     for (int oz = 0; oz < 3; ++oz) {
-                        const int id1 = ctx.cell_seg[cbase - ((long long)ox * P1 + oy) * P2 - oz];
-                        if (id1) {
+                        const long long ci = cbase - ((long long)ox * P1 + oy) * P2 - oz;
+                        const int id1 = MPM_INB(ci, ctx.n_keys, 6) ? ctx.cell_seg[ci] : 0;
+                        const long long si = (long long)(9 * ox + 3 * oy + oz) * cap + (id1 - 1);
+                        if (id1 && MPM_INB(si, 27 * cap, 5)) {
                             R v[4];
-                            load_sum(S, (long long)(9 * ox + 3 * oy + oz) * cap + (id1 - 1), v);
+                            load_sum(S, si, v);
                             acc[0] += v[0]; acc[1] += v[1]; acc[2] += v[2]; acc[3] += v[3];
                         }
                     }
             const long long didx = ax.node_begin + ((long long)i * sc.shape[1] + j) * sc.shape[2] + k;
+            if (!(MPM_INB(didx, ctx.n_nodes, 7) && MPM_INB(gidx, ctx.grid_nodes, 8))) continue;
             R rec[4] = {R(0), R(0), R(0), R(0)};
             if constexpr (MODE == 0) {
                 const R m = acc[0];
@@ -783,7 +800,8 @@ struct DenseStencil {
 __device__ __forceinline__ void unmark_cell(const Ctx& ctx, const SceneAux& ax, const unsigned* __restrict__ skeys,
                                             long long sidx) {
     unsigned k = skeys[sidx];
-    if ((sidx == 0 || skeys[sidx - 1] != k) && (long long)k - ax.cell_begin < ax.ncells) ctx.cell_seg[k] = 0;
+    if ((sidx == 0 || skeys[sidx - 1] != k) && (long long)k - ax.cell_begin < ax.ncells && MPM_INB(k, ctx.n_keys, 2))
+        ctx.cell_seg[k] = 0;
 }
 
 // ---------------------------------------------------------------------------
@@ -797,6 +815,7 @@ g2p_kernel(Ctx ctx, Tape<R> tp, MpmParticles in, MpmParticles out, int advect, u
     long long sidx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (sidx >= ctx.n) return;
     long long p = tp.perm[sidx];
+    if (!MPM_INB(p, ctx.n, 9)) return;
     const int s = ctx.scene_of[sidx];
     const MpmScene& sc = ctx.scenes[s];
     const SceneAux& ax = ctx.aux[s];
@@ -827,6 +846,7 @@ g2p_kernel(Ctx ctx, Tape<R> tp, MpmParticles in, MpmParticles out, int advect, u
             for (int c = 0; c < 3; ++c) {
                 if (!st.vz[c]) continue;
                 R g[4];
+                if (!MPM_INB(rab + st.oz[c], ctx.n_nodes, 7)) continue;
                 load_node(dense, rab + st.oz[c], g);
 #pragma unroll
                 for (int i = 0; i < 3; ++i) {
@@ -899,6 +919,7 @@ bwd_particle_kernel(Ctx ctx, Tape<R> tp, MpmParticles in, const R* __restrict__ 
     long long sidx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (sidx >= ctx.n) return;
     long long p = tp.perm[sidx];
+    if (!MPM_INB(p, ctx.n, 9)) return;
     const int s = ctx.scene_of[sidx];
     const MpmScene& sc = ctx.scenes[s];
     const SceneAux& ax = ctx.aux[s];
@@ -996,6 +1017,7 @@ bwd_particle_kernel(Ctx ctx, Tape<R> tp, MpmParticles in, const R* __restrict__ 
             for (int cc = 0; cc < 3; ++cc) {
                 if (!st.vz[cc]) continue;
                 R gf[4], gb[4];
+                if (!MPM_INB(rab + st.oz[cc], ctx.n_nodes, 7)) continue;
                 load_node(dfw, rab + st.oz[cc], gf);
                 load_node(dbw, rab + st.oz[cc], gb);
                 const R* gv = gf + 1;

@@ -148,7 +148,7 @@ radix_scatter_kernel(const unsigned* __restrict__ keys_in, const unsigned* __res
             if (rank == 0) base = wcnt[warp][dig];
         }
         base = __shfl_sync(0xffffffffu, base, leader);
-        if (valid) {
+        if (valid && MPM_INB((long long)base + rank, n, 10)) {
             keys_out[base + rank] = key[r];
             vals_out[base + rank] = val[r];
         }

@@ -142,3 +142,18 @@ def test_rollout_workspace_layout():
     assert lib.mpm_rollout_fwd(h, 16, None, 3, 0, 1, None, 4096, None) == L.MPM_ERR_ARG
     assert lib.mpm_rollout_bwd(h, None, 16, 3, 0, 1, None, 4096, None, None, None, None) == L.MPM_ERR_ARG
     lib.mpm_plan_destroy(h)
+
+
+def test_checked_build_exports_the_same_abi():
+    """The bounds-checked library (MPM_CHECK_BOUNDS) exports exactly the
+    release library's entry points; the release library reports that it has
+    no checks."""
+    from morphompm_b200 import build as B
+    lib = L.load()
+    cnt, site, idx = C.c_int64(5), C.c_int32(5), C.c_int64(5)
+    assert lib.mpm_check_violations(C.byref(cnt), C.byref(site), C.byref(idx), None) == L.MPM_ERR_UNSUPPORTED
+    assert (cnt.value, site.value, idx.value) == (0, 0, -1)
+    path = B.build(checked=True)
+    syms = lambda p: set(re.findall(r"\bT (mpm_\w+)", subprocess.run(["nm", "-D", "--defined-only", p],
+                                                                     capture_output=True, text=True).stdout))
+    assert syms(path) == syms(L.lib_path()) == set(declared())

@@ -56,6 +56,7 @@ struct MpmPlan {
     // the state whose keys and P2G records the last MPM_FWD_EMIT call formed
     bool chain_valid = false;
     int chain_t = 0;
+    bool tile_flags_pending = false;   // an emitting G2P flagged the next step's tiles
     MpmParticles chain_state{};
     size_t ws_bytes = 0;
     // tape offsets
@@ -110,6 +111,8 @@ Ctx make_ctx(MpmPlan* P) {
     c.n_scenes = (int)P->scenes.size();
     c.tile_xy = P->tune.tile_xy;
     c.tile_z = P->tune.tile_z;
+    c.tile_xy_shift = P->tune.tile_xy == 16 ? 4 : (P->tune.tile_xy == 8 ? 3 : 2);
+    c.tile_z_shift = P->tune.tile_z == 16 ? 4 : (P->tune.tile_z == 8 ? 3 : 2);
     c.active_cap = P->active_cap;
     c.gap_thresh = P->tune.fp64_gap_thresh < 0 ? 0.0f : P->tune.fp64_gap_thresh;
     return c;
@@ -177,9 +180,9 @@ inline int check_launch() {
 }
 
 // segment table of the sorted keys (and, in the forward, the active tile flags)
-int build_segments(MpmPlan* P, const Ctx& ctx, const unsigned* skeys, int flag_tiles, cudaStream_t st) {
+int build_segments(MpmPlan* P, const Ctx& ctx, const unsigned* skeys, cudaStream_t st) {
     Site site(P, MPM_K_MARK, 3, st);
-    seg_count_kernel<<<P->nblk_seg, SEG_THREADS, 0, st>>>(ctx, skeys, flag_tiles);
+    seg_count_kernel<<<P->nblk_seg, SEG_THREADS, 0, st>>>(ctx, skeys);
     scan_counts_kernel<<<1, 1024, 0, st>>>(ctx.blk_count, P->nblk_seg, ctx.n_seg, INT_MAX, ctx.status);
     seg_write_kernel<<<P->nblk_seg, SEG_THREADS, 0, st>>>(ctx, skeys);
     return check_launch();
@@ -277,7 +280,7 @@ int step_fwd_R(MpmPlan* P, const MpmParticles& in, MpmParticles& out, int advect
     if (!chained) { Site s(P, MPM_K_BIN, 1, st); bin_kernel<R><<<g, B, 0, st>>>(ctx, in, keys); }
     int rc = run_sort(P, keys, tp.skeys, tp.perm, st);
     if (rc) return rc;
-    rc = build_segments(P, ctx, tp.skeys, 1, st);
+    rc = build_segments(P, ctx, tp.skeys, st);
     if (rc) return rc;
     {
         Site s(P, MPM_K_COMPACT, 3, st);
@@ -665,11 +668,19 @@ int mpm_step_fwd_chain(MpmPlan* P, const MpmParticles* in, MpmParticles* out, in
             std::memcmp(&P->chain_state, in, sizeof(MpmParticles)) != 0)
             return MPM_ERR_ARG;
     }
-    P->chain_valid = false;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
+    // the active-tile flags of the next step are set where its keys are formed
+    // (bin or an emitting G2P); an emitted state that is not continued leaves
+    // its flags behind, so they are cleared before binning another state
+    if (P->tile_flags_pending && !(flags & MPM_FWD_CHAINED) &&
+        cudaMemsetAsync(P->ws + P->o_tile_flag, 0, (size_t)P->n_tiles * 4, st) != cudaSuccess)
+        return MPM_ERR_CUDA;
+    P->chain_valid = false;
+    P->tile_flags_pending = false;
     int rc = P->real_bytes == 4 ? step_fwd_R<float>(P, *in, *out, advect, step_index, tp, flags, st)
                                 : step_fwd_R<double>(P, *in, *out, advect, step_index, tp, flags, st);
     if (rc == MPM_OK && (flags & MPM_FWD_EMIT)) {
+        P->tile_flags_pending = true;
         P->chain_valid = true;
         P->chain_t = step_index + 1;
         P->chain_state = *out;

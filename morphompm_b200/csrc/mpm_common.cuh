@@ -79,6 +79,8 @@ struct Ctx {
     int n_scenes;
     int tile_xy;
     int tile_z;
+    int tile_xy_shift;           // log2 of the tile edges (tiles are 4, 8 or 16 nodes)
+    int tile_z_shift;
     int active_cap;              // capacity of a tape's active-tile list
     float gap_thresh;            // FP32 Hencky FP64-fallback threshold (relative sv gap)
 };

@@ -118,12 +118,36 @@ __device__ __forceinline__ void load_Fg(const Ctx& ctx, const MpmScene& sc, cons
 // ---------------------------------------------------------------------------
 // cell key of a particle at x (its padded stencil-base cell, or the scene's
 // "outside" key) and its fractional position fx in the stencil
+// Active tiles of the next step: the node tiles that the stencil of a particle
+// inside the grid touches (nodes base..base+2 clipped to the grid), flagged
+// where its cell key is formed.  Every particle of an occupied cell flags the
+// same tiles; the flags are plain stores of 1.
+__device__ __forceinline__ void flag_stencil_tiles(const Ctx& ctx, const MpmScene& sc, const SceneAux& ax,
+                                                   const int base[3]) {
+    int tlo[3], thi[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        const int sh = d == 2 ? ctx.tile_z_shift : ctx.tile_xy_shift;
+        const int lo = base[d] < 0 ? 0 : base[d];
+        const int hi = base[d] + 2 > sc.shape[d] - 1 ? sc.shape[d] - 1 : base[d] + 2;
+        tlo[d] = lo >> sh;
+        thi[d] = hi >> sh;
+    }
+    for (int a = tlo[0]; a <= thi[0]; ++a)
+        for (int b = tlo[1]; b <= thi[1]; ++b)
+            for (int e = tlo[2]; e <= thi[2]; ++e) {
+                const long long ti = ax.tile_begin + ((long long)a * ax.ntile[1] + b) * ax.ntile[2] + e;
+                if (MPM_INB(ti, ctx.n_tiles, 1)) ctx.tile_flag[ti] = 1;
+            }
+}
+
 template <typename R>
 __device__ __forceinline__ unsigned particle_key(const Ctx& ctx, const MpmScene& sc, const SceneAux& ax,
                                                  const R x[3], R fx[3]) {
     int base[3];
     const bool inside = bin_particle(x, (R)(1.0 / sc.dx), sc.shape, base, fx);
     if (inside) {
+        flag_stencil_tiles(ctx, sc, ax, base);
         long long c = ((long long)(base[0] + 2) * (sc.shape[1] + 2) + (base[1] + 2)) * (sc.shape[2] + 2) + (base[2] + 2);
         return (unsigned)(ax.cell_begin + c);
     }
@@ -157,7 +181,7 @@ __global__ void bin_keys_single(MpmScene sc, long long n, const R* __restrict__ 
 
 // ---------------------------------------------------------------------------
 // segment tables: one segment per occupied cell (a run of equal sorted keys).
-// Three kernels: per-block counts of segment starts (and tile flags), a
+// Three kernels: per-block counts of segment starts, a
 // single-block scan of the counts, and the writes of seg_first / seg_last /
 // cell_seg with each slot's segment id from the scan.  "Outside" keys (stencil
 // entirely off the grid) form no segment.
@@ -165,14 +189,6 @@ __global__ void bin_keys_single(MpmScene sc, long long n, const R* __restrict__ 
 constexpr int SEG_THREADS = 256;
 constexpr int SEG_ITEMS = 16;
 constexpr int SEG_TILE = SEG_THREADS * SEG_ITEMS;
-
-__device__ __forceinline__ void decode_cell(const MpmScene& sc, long long c, int cell[3]) {
-    const unsigned P1 = sc.shape[1] + 2, P2 = sc.shape[2] + 2, u = (unsigned)c;
-    const unsigned r = u / P2;
-    cell[2] = (int)(u - r * P2);
-    cell[1] = (int)(r % P1);
-    cell[0] = (int)(r / P1);
-}
 
 // is slot s the start of an inside segment?
 __device__ __forceinline__ bool seg_start(const Ctx& ctx, const unsigned* __restrict__ skeys, long long s,
@@ -182,35 +198,10 @@ __device__ __forceinline__ bool seg_start(const Ctx& ctx, const unsigned* __rest
     return (long long)k - ax.cell_begin < ax.ncells;
 }
 
-__device__ __forceinline__ void flag_tiles(const Ctx& ctx, long long s, unsigned k) {
-    const int sc_i = ctx.scene_of[s];
-    const MpmScene& sc = ctx.scenes[sc_i];
-    const SceneAux& ax = ctx.aux[sc_i];
-    int cell[3];
-    decode_cell(sc, (long long)k - ax.cell_begin, cell);
-    int tlo[3], thi[3];
-    const int T[3] = {ctx.tile_xy, ctx.tile_xy, ctx.tile_z};
-#pragma unroll
-    for (int d = 0; d < 3; ++d) {
-        int b = cell[d] - 2;
-        int lo = b < 0 ? 0 : b;
-        int hi = b + 2 > sc.shape[d] - 1 ? sc.shape[d] - 1 : b + 2;
-        tlo[d] = lo / T[d];
-        thi[d] = hi / T[d];
-    }
-    for (int a = tlo[0]; a <= thi[0]; ++a)
-        for (int b = tlo[1]; b <= thi[1]; ++b)
-            for (int e = tlo[2]; e <= thi[2]; ++e)
-            {
-                const long long ti = ax.tile_begin + ((long long)a * ax.ntile[1] + b) * ax.ntile[2] + e;
-                if (MPM_INB(ti, ctx.n_tiles, 1)) ctx.tile_flag[ti] = 1;
-            }
-}
-
 // Slots of a block are visited warp-striped (slot = block base + round*256 +
 // thread), so every load of the sorted keys is coalesced.
 __global__ void __launch_bounds__(SEG_THREADS)
-seg_count_kernel(Ctx ctx, const unsigned* __restrict__ skeys, int flag) {
+seg_count_kernel(Ctx ctx, const unsigned* __restrict__ skeys) {
     __shared__ unsigned red[SEG_THREADS / 32];
     const long long base = (long long)blockIdx.x * SEG_TILE;
     unsigned cnt = 0;
@@ -219,10 +210,7 @@ seg_count_kernel(Ctx ctx, const unsigned* __restrict__ skeys, int flag) {
         long long s = base + (long long)r * SEG_THREADS + threadIdx.x;
         if (s >= ctx.n) break;
         unsigned k = skeys[s];
-        if (seg_start(ctx, skeys, s, k)) {
-            ++cnt;
-            if (flag) flag_tiles(ctx, s, k);
-        }
+        if (seg_start(ctx, skeys, s, k)) ++cnt;
     }
     for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
     if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = cnt;

@@ -146,10 +146,15 @@ __device__ __forceinline__ unsigned particle_key(const Ctx& ctx, const MpmScene&
                                                  const R x[3], R fx[3]) {
     int base[3];
     const bool inside = bin_particle(x, (R)(1.0 / sc.dx), sc.shape, base, fx);
+    // the lanes of a warp in the same cell flag the same tiles: one of them does
+    const long long cell = ((long long)(base[0] + 2) * (sc.shape[1] + 2) + (base[1] + 2)) * (sc.shape[2] + 2) +
+                           (base[2] + 2);
+    const unsigned tag = inside ? (unsigned)(ax.cell_begin + cell) : 0xffffffffu;
+    const unsigned peers = __match_any_sync(__activemask(), tag);
+    const bool leader = (peers & ((1u << (threadIdx.x & 31)) - 1u)) == 0u;
     if (inside) {
-        flag_stencil_tiles(ctx, sc, ax, base);
-        long long c = ((long long)(base[0] + 2) * (sc.shape[1] + 2) + (base[1] + 2)) * (sc.shape[2] + 2) + (base[2] + 2);
-        return (unsigned)(ax.cell_begin + c);
+        if (leader) flag_stencil_tiles(ctx, sc, ax, base);
+        return tag;
     }
     raise_status(ctx.status, MPM_WARN_OUTSIDE);
     return (unsigned)(ax.cell_begin + ax.ncells);

@@ -78,7 +78,18 @@ def _check(plan: Plan):
             raise L.MpmError(st, "step")
 
 
+def _check_shapes(state: ParticleState):
+    """x, v: (n, 3); C, F, Fg: (n, 3, 3) -- the reference's layout (state.py:11-21)."""
+    n = tuple(state.x.shape)[0] if len(tuple(state.x.shape)) == 2 else None
+    want = {"x": (n, 3), "v": (n, 3), "C": (n, 3, 3), "F": (n, 3, 3), "Fg": (n, 3, 3)}
+    for k, w in want.items():
+        got = tuple(getattr(state, k).shape)
+        if n is None or got != w:
+            raise ValueError(f"ParticleState.{k} has shape {got}, expected {w if n is not None else '(n, 3)'}")
+
+
 def step(state: ParticleState, model, cfg, advect=True, t: int = 0):
+    _check_shapes(state)
     ref = state.x
     x = to_device(state.x).contiguous()
     dev, dt = x.device, x.dtype

@@ -1,0 +1,20 @@
+"""transfer.step refuses a mis-shaped particle state before any device work
+(no GPU needed for the refusal)."""
+import numpy as np
+import pytest
+
+from morphompm_b200 import transfer
+from morphompm_b200.config import Material, SimConfig
+from morphompm_b200.constitutive import NeoHookean
+from morphompm_b200.state import ParticleState
+
+
+@pytest.mark.parametrize("field,shape", [("x", (5, 2)), ("v", (4, 3)), ("C", (5, 9)), ("F", (5, 3, 2)),
+                                         ("Fg", (6, 3, 3))])
+def test_misshaped_state_is_refused(field, shape):
+    n = 5
+    st = dict(x=np.zeros((n, 3)), v=np.zeros((n, 3)), C=np.zeros((n, 3, 3)), F=np.tile(np.eye(3), (n, 1, 1)),
+              Fg=np.tile(np.eye(3), (n, 1, 1)))
+    st[field] = np.zeros(shape)
+    with pytest.raises(ValueError, match=field):
+        transfer.step(ParticleState(**st), NeoHookean(Material()), SimConfig())

@@ -172,3 +172,26 @@ def test_free_swell_and_cpp_parity_scene(golden):
     st, _ = integrate.rollout(integrate.iso_growth_state(g["parity27_pts"], 1.05), _models()["hencky"], cfg, 30,
                               advect=True)
     assert rel(st.F, g["parity27_F"]) < 1e-11
+
+
+def test_confined_swell_gate_on_device():
+    """constitutive.py:155-179 through the device stress (FP64): the root of
+    tau_zz for a laterally confined swelling block, and tau_xx there, equal the
+    oracle's and the reference's 2.0028 / -5147.403."""
+    from oracle import mpm_oracle as O
+    m = _models()["nh"]
+    om = O.Model.elastic("nh", 1e4, 0.3)
+    Fg = 1.5 * np.eye(3)
+    lo, hi = 1.0, 4.0
+    for _ in range(200):
+        mid = 0.5 * (lo + hi)
+        if m.stress(np.diag([1.0, 1.0, mid]), Fg)[2, 2] > 0:
+            hi = mid
+        else:
+            lo = mid
+    lam = 0.5 * (lo + hi)
+    tau = m.stress(np.diag([1.0, 1.0, lam]), Fg)
+    assert abs(lam - 2.0028) < 5e-5
+    assert abs(tau[0, 0] - (-5147.403)) < 1e-3
+    otau = O.stress(om, np.diag([1.0, 1.0, lam])[None], Fg[None])[0]
+    assert np.max(np.abs(tau - otau)) < 1e-12 * 5147.403

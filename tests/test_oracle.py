@@ -173,3 +173,27 @@ def test_oracle_vs_live_reference():
         assert rel(ns_o.F, ns_r.F) < 1e-13 and rel(ns_o.x, ns_r.x) < 1e-15
         for a, b in zip(g_o, g_r):
             assert rel(a, b) < 1e-12
+
+
+def _confined_root(tau_zz, lo=1.0, hi=4.0, it=200):
+    """Bisection for tau_zz(lam) = 0 (tau_zz increasing in lam)."""
+    for _ in range(it):
+        mid = 0.5 * (lo + hi)
+        if tau_zz(mid) > 0:
+            hi = mid
+        else:
+            lo = mid
+    return 0.5 * (lo + hi)
+
+
+def test_confined_swell_gate():
+    """The reference's confined-swell check (constitutive.py:155-179): neo-Hookean,
+    E = 1e4, nu = 0.3, Fg = 1.5 I, laterally confined F = diag(1, 1, lam);
+    tau_zz(lam*) = 0 at lam* = 2.0028 with tau_xx = -5147.403."""
+    m = O.Model.elastic("nh", 1e4, 0.3)
+    Fg = 1.5 * np.eye(3)[None]
+    tau = lambda lam: O.stress(m, np.diag([1.0, 1.0, lam])[None], Fg)[0]
+    lam = _confined_root(lambda l: tau(l)[2, 2])
+    assert abs(lam - 2.0028) < 5e-5
+    assert abs(tau(lam)[0, 0] - (-5147.403)) < 1e-3
+    assert abs(tau(lam)[2, 2]) < 1e-9

@@ -13,7 +13,6 @@ trajectories of the actual batch for each candidate on the current GPU.
 """
 from __future__ import annotations
 
-import itertools
 import json
 import os
 import time

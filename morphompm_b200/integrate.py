@@ -21,7 +21,7 @@ import numpy as np
 import torch
 
 from .devarray import like_input, to_device
-from .runtime import SLAB_ROWS, ROW_C, ROW_F, ROW_V, ROW_X
+from .runtime import SLAB_ROWS, ROW_F, ROW_X
 from .state import ParticleState
 from .constitutive import is_external
 from .layout import cell_order_device

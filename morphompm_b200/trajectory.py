@@ -16,7 +16,7 @@ forward+adjoint can be captured once in a CUDA graph and replayed
 from __future__ import annotations
 
 import math
-from typing import List, Optional
+from typing import Optional
 
 import torch
 

@@ -20,8 +20,6 @@ from __future__ import annotations
 
 import os
 from collections import OrderedDict
-from dataclasses import astuple
-from typing import Optional
 
 import torch
 

@@ -327,8 +327,9 @@ def main():
     units = n_tot * a.mpm_steps * world
     value = units / (ms_per / 1e3)
 
-    # end to end through the public API: pinned host slab -> device, trajectory,
-    # per-scene loss and dL/dg back to the host
+    # end to end through the public API: every step copies its pinned host slab
+    # to the device (on a side stream, overlapping the previous trajectory),
+    # runs the trajectory and reads the per-scene loss and dL/dg back
     loss_h = torch.empty(len(scn), dtype=torch.float64).pin_memory()
     grad_h = torch.empty(len(scn), dtype=torch.float64).pin_memory()
     torch.cuda.synchronize()
@@ -336,7 +337,7 @@ def main():
         dist.barrier()
     e0.record(s)
     for _ in range(a.steps):
-        b.load(slab_h, non_blocking=True)
+        b.prefetch(slab_h)
         b.replay()
         loss_h.copy_(b.loss, non_blocking=True)
         grad_h.copy_(b.dloss_dg, non_blocking=True)

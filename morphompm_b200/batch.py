@@ -123,6 +123,8 @@ class Batch:
             self.order_dev = torch.as_tensor(self.order).to(dev)
             self.inverse_dev = torch.as_tensor(np.argsort(self.order)).to(dev)
             self._stage = torch.empty(SLAB_ROWS, self.n, dtype=dtype, device=dev)
+        self._copy_stream = None      # prefetch(): side-stream input copies
+        self._pending = False
         self.graph = None
 
     @staticmethod
@@ -161,6 +163,39 @@ class Batch:
             self._stage.copy_(src, non_blocking=non_blocking)
             torch.index_select(self._stage, 1, self.order_dev, out=self.slab0)
 
+    def prefetch(self, slab_host):
+        """Start the host -> device copy of the next trajectory's (24, n) host
+        slab (pinned) on a side stream, so that it overlaps the trajectory that
+        is running; the next run() / replay() waits for it and moves it into
+        the input, in the batch's cell order.  The host slab must stay
+        unchanged until that run starts."""
+        src = torch.from_numpy(slab_host) if isinstance(slab_host, np.ndarray) else slab_host
+        dev = self.plan.device
+        if self._copy_stream is None:
+            self._copy_stream = torch.cuda.Stream(device=dev)
+            self._inbox = torch.empty(SLAB_ROWS, self.n, dtype=self.dtype, device=dev)
+            self._inbox_ready = torch.cuda.Event()
+            self._inbox_free = torch.cuda.Event()
+            self._inbox_free.record(torch.cuda.current_stream(dev))
+        cs = self._copy_stream
+        cs.wait_event(self._inbox_free)          # the previous prefetch has been taken
+        with torch.cuda.stream(cs):
+            self._inbox.copy_(src, non_blocking=True)
+            self._inbox_ready.record(cs)
+        self._pending = True
+
+    def _take_prefetched(self):
+        if not self._pending:
+            return
+        cur = torch.cuda.current_stream(self.plan.device)
+        cur.wait_event(self._inbox_ready)
+        if self.order is None:
+            self.slab0.copy_(self._inbox)
+        else:
+            torch.index_select(self._inbox, 1, self.order_dev, out=self.slab0)
+        self._inbox_free.record(cur)
+        self._pending = False
+
     def _to_input_order(self, slab: torch.Tensor) -> torch.Tensor:
         if self.order is None:
             return slab
@@ -176,6 +211,7 @@ class Batch:
         return self._to_input_order(self.rollout.bar0)
 
     def run(self):
+        self._take_prefetched()
         return self.rollout.run(self.slab0)
 
     def capture(self, pre_capture=None):
@@ -183,6 +219,7 @@ class Batch:
         return self.graph
 
     def replay(self):
+        self._take_prefetched()
         if self.graph is None:
             self.capture()
         self.graph.replay()

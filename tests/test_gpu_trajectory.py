@@ -197,3 +197,29 @@ def test_save_batch_writes_each_scene(tmp_path):
         np.testing.assert_array_equal(st.F.reshape(k, 9), fin[15:24, p0:p0 + k].T)
         assert np.allclose(st.Fg, (1.0 + sc[s]["growth_A"]) * np.eye(3))
         p0 += k
+
+
+def test_prefetch_matches_load():
+    """Batch.prefetch (side-stream input copy overlapping the running
+    trajectory) feeds each replay exactly the slab a blocking load would."""
+    from morphompm_b200.batch import Batch, host_slab
+    scn = _small_batch_scenes()
+    b = Batch(scn, 5, dtype=torch.float32)
+    s1 = host_slab(scn)
+    s2 = s1.copy()
+    s2[0:3] += 0.002
+    pins = [torch.from_numpy(s).pin_memory() for s in (s1, s2)]
+    ref = []
+    for p in pins:
+        b.load(p, non_blocking=False)
+        b.replay()
+        ref.append(b.loss.clone())
+    got = []
+    for i in (0, 1, 0, 1):
+        b.prefetch(pins[i])
+        b.replay()
+        got.append(b.loss.clone())
+    torch.cuda.synchronize()
+    assert not torch.equal(ref[0], ref[1])
+    for i, g in zip((0, 1, 0, 1), got):
+        assert torch.equal(g, ref[i])

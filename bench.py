@@ -321,10 +321,12 @@ def main():
     ms = e0.elapsed_time(e1)
     clk = clocks.stop()
     prof = plan.profile_end()
-    from morphompm_b200.shard import max_over_ranks
+    from morphompm_b200.shard import max_over_ranks, sum_over_ranks
     ms = max_over_ranks(ms, dev)
     ms_per = ms / a.steps
-    units = n_tot * a.mpm_steps * world
+    # every rank runs a batch of its own (its own seed): the job's particles are the sum
+    n_all = int(sum_over_ranks(n_tot, dev))
+    units = n_all * a.mpm_steps
     value = units / (ms_per / 1e3)
 
     # end to end through the public API: every step copies its pinned host slab
@@ -381,7 +383,7 @@ def main():
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
             "ms_per_step": ms_per, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "scenes": len(scn), "particles": n_tot * world,
+            "config": {"workload": WORKLOAD, "scenes": len(scn), "particles": n_all,
                        "mpm_steps": a.mpm_steps, "ckpt_every": k, "l2": "inputs larger than L2 "
                        f"({n_tot * 24 * 4 / 1e6:.0f} MB state per GPU)", "schedule": plan.tuning or "defaults",
                        "parallelism": f"{world} independent batches (no collective)"},

@@ -22,6 +22,19 @@ def lpt_assign(costs: Sequence[float], world: int) -> List[List[int]]:
     return [sorted(x) for x in out]
 
 
+def sum_over_ranks(value: float, device=None) -> float:
+    """Sum of a per-rank float over the default process group (identity when
+    torch.distributed is not initialised): e.g. the particles all ranks
+    processed, when every rank runs a batch of its own."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return float(value)
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device or "cpu")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
 def max_over_ranks(value: float, device=None) -> float:
     """Max of a per-rank float over the default process group (identity when
     torch.distributed is not initialised)."""

@@ -111,4 +111,6 @@ def rollout_loss(x0, growth, model, cfg, n_steps: int, advect: bool = True, loss
     functional as ``integrate.dloss_dg``, differentiable in x0 and growth."""
     if not isinstance(growth, torch.Tensor):
         growth = torch.tensor(float(growth), dtype=x0.dtype, device=x0.device)
+    if ckpt_every is None:
+        ckpt_every = getattr(cfg, "checkpoint_every", None)
     return _RolloutLoss.apply(x0, growth, model, cfg, int(n_steps), bool(advect), loss, x_obs, ckpt_every)

@@ -4,7 +4,11 @@
 Optional fields extend it for the B200 path without changing any default:
 a non-cubic ``shape`` (defaults to (N, N, N)), sticky ``wall`` nodes, a sticky
 ``clamp`` box, ``gravity`` and the grid-mass threshold ``mass_eps``
-(transfer.py:56 uses 1e-12).
+(transfer.py:56 uses 1e-12); the arithmetic type ``dtype`` ("float32" or
+"float64"; default: that of the inputs, numpy arrays run in float64), the
+CUDA ``device`` (default: the inputs' or the current one) and
+``checkpoint_every`` (default: keep every step) of the trajectory gradients.
+The JSON config files keep the reference's fields only (io.py:98-111).
 """
 from __future__ import annotations
 
@@ -42,6 +46,9 @@ class SimConfig:
     clamp_hi: Sequence[int] = (0, 0, 0)
     gravity: Sequence[float] = (0.0, 0.0, 0.0)
     mass_eps: float = 1.0e-12
+    dtype: Optional[str] = None
+    device: Optional[str] = None
+    checkpoint_every: Optional[int] = None
 
     @property
     def inv_dx(self) -> float:
@@ -58,3 +65,19 @@ class SimConfig:
     @property
     def grid_shape(self) -> Tuple[int, int, int]:
         return tuple(self.shape) if self.shape is not None else (self.N, self.N, self.N)
+
+
+_DTYPES = ("float32", "float64")
+
+
+def compute_target(cfg):
+    """(torch dtype or None, device or None) that ``cfg`` asks the device path
+    to compute in; None leaves the choice to the inputs.  Configs without the
+    extension fields (the reference's own SimConfig) ask for nothing."""
+    dt = getattr(cfg, "dtype", None)
+    if dt is not None and dt not in _DTYPES:
+        raise ValueError(f"SimConfig.dtype must be one of {_DTYPES} or None, not {dt!r}")
+    if dt is not None:
+        import torch
+        dt = getattr(torch, dt)
+    return dt, getattr(cfg, "device", None)

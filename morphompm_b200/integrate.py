@@ -24,19 +24,20 @@ from .devarray import like_input, to_device
 from .runtime import SLAB_ROWS, ROW_F, ROW_X
 from .state import ParticleState
 from .constitutive import is_external
+from .config import compute_target
 from .layout import cell_order_device
 from .transfer import get_plan, scene_spec, step, step_vjp
 
 
-def _dev_state(state0: ParticleState) -> ParticleState:
-    x = to_device(state0.x).contiguous()
+def _dev_state(state0: ParticleState, cfg=None) -> ParticleState:
+    x = to_device(state0.x, *compute_target(cfg)).contiguous()
     dt, dev = x.dtype, x.device
     return ParticleState(x, *(to_device(a, dt, dev).contiguous() for a in (state0.v, state0.C, state0.F, state0.Fg)))
 
 
 def rollout(state0: ParticleState, model, cfg, n_steps, advect=False):
     ref = state0.x
-    st = _dev_state(state0)
+    st = _dev_state(state0, cfg)
     caches = []
     for t in range(n_steps):
         st, cache = step(st, model, cfg, advect=advect)
@@ -99,7 +100,9 @@ def dloss_dg(pts, model, cfg, g, n_steps, advect, loss: str = "detF", x_obs=None
     from .trajectory import Rollout
     if is_external(model):
         return _dloss_dg_steps(pts, model, cfg, g, n_steps, advect, loss, x_obs)
-    p = to_device(pts).contiguous()
+    if ckpt_every is None:
+        ckpt_every = getattr(cfg, "checkpoint_every", None)
+    p = to_device(pts, *compute_target(cfg)).contiguous()
     n = p.shape[0]
     if n == 0:
         return 0.0, 0.0     # no particles: sum det F over none
@@ -127,7 +130,7 @@ def _dloss_dg_steps(pts, model, cfg, g, n_steps, advect, loss, x_obs):
     """dloss_dg through the single-step API (per-step caches, as the
     reference's rollout / rollout_vjp): the path of user-defined materials,
     whose stress is a callback evaluated every step."""
-    p = to_device(pts).contiguous()
+    p = to_device(pts, *compute_target(cfg)).contiguous()
     n = p.shape[0]
     if n == 0:
         return 0.0, 0.0
@@ -171,7 +174,9 @@ def dloss_dparams(pts, model, cfg, g, n_steps, advect, loss: str = "detF", x_obs
     from .trajectory import Rollout
     if is_external(model):
         raise TypeError("material-parameter gradients need a built-in elastic model (mu, lambda)")
-    p = to_device(pts).contiguous()
+    if ckpt_every is None:
+        ckpt_every = getattr(cfg, "checkpoint_every", None)
+    p = to_device(pts, *compute_target(cfg)).contiguous()
     n = p.shape[0]
     if n == 0:
         return 0.0, {"g": 0.0, "mu": 0.0, "lam": 0.0, "E": 0.0, "nu": 0.0}

@@ -25,6 +25,7 @@ import torch
 
 from . import _lib as L
 from .constitutive import is_external, model_fields
+from .config import compute_target
 from .devarray import like_input, to_device
 from .runtime import Plan, SceneSpec, aos_cotangents, aos_particles
 from .state import ParticleState
@@ -89,7 +90,8 @@ def _check_shapes(state: ParticleState):
 def step(state: ParticleState, model, cfg, advect=True, t: int = 0):
     _check_shapes(state)
     ref = state.x
-    x = to_device(state.x).contiguous()
+    want_dt, want_dev = compute_target(cfg)
+    x = to_device(state.x, want_dt, want_dev).contiguous()
     dev, dt = x.device, x.dtype
     v = to_device(state.v, dt, dev).contiguous()
     Cm = to_device(state.C, dt, dev).contiguous()

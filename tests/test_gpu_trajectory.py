@@ -223,3 +223,29 @@ def test_prefetch_matches_load():
     assert not torch.equal(ref[0], ref[1])
     for i, g in zip((0, 1, 0, 1), got):
         assert torch.equal(g, ref[i])
+
+
+def test_config_dtype_and_checkpoint_fields():
+    """SimConfig(dtype="float32") runs numpy inputs on the FP32 path (the
+    result of passing FP32 tensors, returned as the input's numpy type);
+    SimConfig(checkpoint_every=k) is the default ckpt_every of dloss_dg."""
+    from morphompm_b200 import integrate, transfer
+    from morphompm_b200.config import Material, SimConfig
+    from morphompm_b200.constitutive import Hencky
+    from morphompm_b200.state import ParticleState
+    rng = np.random.default_rng(6)
+    n = 40
+    x = rng.uniform(0.3, 0.6, size=(n, 3))
+    F = np.eye(3) + 0.02 * rng.standard_normal((n, 3, 3))
+    st = ParticleState(x, 0.05 * rng.standard_normal((n, 3)), 0.1 * rng.standard_normal((n, 3, 3)), F,
+                       1.1 * np.tile(np.eye(3), (n, 1, 1)))
+    base = dict(N=12, dx=1 / 12, dt=4e-4, sp=1 / 24, material=Material(E=1e4, nu=0.3))
+    m = Hencky(Material(E=1e4, nu=0.3))
+    ns, _ = transfer.step(st, m, SimConfig(dtype="float32", **base))
+    f32 = lambda a: torch.as_tensor(a, dtype=torch.float32, device="cuda")
+    ref, _ = transfer.step(ParticleState(*(f32(a) for a in (st.x, st.v, st.C, st.F, st.Fg))), m, SimConfig(**base))
+    assert isinstance(ns.F, np.ndarray) and ns.F.dtype == np.float64
+    assert np.array_equal(ns.F, ref.F.double().cpu().numpy())
+    a = integrate.dloss_dg(x, m, SimConfig(checkpoint_every=2, **base), 1.1, 5, True)
+    b = integrate.dloss_dg(x, m, SimConfig(**base), 1.1, 5, True, ckpt_every=2)
+    assert a == b

@@ -109,6 +109,9 @@ typedef struct MpmTuning {
 
 typedef struct MpmPlan MpmPlan;   /* host-side plan (offsets, tile tables)         */
 
+/* ---- plans: no counterpart in the reference, whose step allocates its grid
+ * and caches as numpy arrays on every call (transfer.py:33-79). ---- */
+
 /* Build a plan for a batch of scenes (host only, no CUDA calls).
  * real_bytes is MPM_F32 or MPM_F64. */
 int mpm_plan_create(const MpmScene* scenes, int32_t n_scenes, int32_t real_bytes,
@@ -172,7 +175,10 @@ int mpm_plan_set_external_stress(MpmPlan* plan, const void* tau, void* tau_bar);
  * mpm_step_fwd_chain calls. */
 int mpm_plan_set_particle_mass(MpmPlan* plan, const void* mass, const void* vol0);
 
-/* Optional per-particle growth field phi_p (growth_mode 1), real type. */
+/* Optional per-particle growth field phi_p (growth_mode 1), real type: the
+ * field growth law g_p(t) = 1 + A ramp(t) phi_p of the reference's growth
+ * drivers (docs/PHASE3_morphogenesis.md:55-57), evaluated on the device; the
+ * reference's own driver sets Fg = g I per call (integrate.py:31-34). */
 int mpm_plan_set_growth_field(MpmPlan* plan, const void* phi);
 
 /* One forward MLS-MPM step for every scene of the batch:
@@ -320,6 +326,7 @@ int mpm_step_fwd_noalloc(const MpmScene* scene, int32_t real_bytes, const MpmPar
  * MPM_ERR_UNSUPPORTED. */
 int mpm_check_violations(int64_t* count, int32_t* first_site, int64_t* first_index, void* stream);
 
+/* ABI version of this header (1). */
 int mpm_version(void);
 
 #ifdef __cplusplus

@@ -157,3 +157,28 @@ def test_checked_build_exports_the_same_abi():
     syms = lambda p: set(re.findall(r"\bT (mpm_\w+)", subprocess.run(["nm", "-D", "--defined-only", p],
                                                                      capture_output=True, text=True).stdout))
     assert syms(path) == syms(L.lib_path()) == set(declared())
+
+
+def test_budget_schedule_covers_the_engine_memory():
+    """The checkpoint interval budget_schedule picks fits: the native engine's
+    workspace (mpm_rollout_workspace_bytes) plus the three slabs Rollout owns
+    (final state, loss seed, initial cotangents) stay within the budget."""
+    from morphompm_b200.trajectory import budget_schedule
+    lib = L.load()
+    n = 5000
+    arr = (L.MpmScene * 1)(_scene(n, 0, (24, 24, 24)))
+    h = C.c_void_p()
+    assert lib.mpm_plan_create(arr, 1, 4, None, C.byref(h)) == 0
+    tb = C.c_size_t()
+    lib.mpm_plan_tape_bytes(h, C.byref(tb))
+    state = 24 * n * 4
+    for steps in (1, 7, 50, 200):
+        for frac in (0.05, 0.3, 1.0, 3.0):
+            budget = int(frac * steps * (state + tb.value))
+            k = budget_schedule(steps, state, tb.value, budget)
+            nb = C.c_size_t()
+            assert lib.mpm_rollout_workspace_bytes(h, steps, k, C.byref(nb)) == 0
+            used = nb.value + 3 * state
+            if k > 1:                     # k = 1 is the floor, taken even when nothing fits
+                assert used <= budget + 8 * 256, (steps, frac, k, used, budget)
+    lib.mpm_plan_destroy(h)

@@ -157,3 +157,35 @@ class PerParticle:
         outs = [self.model.stress_vjp(Fh[p], Fgh[p], Ch[p], tb[p]) for p in range(Fh.shape[0])]
         return tuple(torch.as_tensor(np.stack([o[k] for o in outs]), dtype=F.dtype, device=F.device)
                      for k in range(3))
+
+
+def confined_swell_neohookean(mat, g: float = 1.5):
+    """Closed-form check of the neo-Hookean model (constitutive.py:150-170):
+    a block growing by Fg = g I, confined laterally (F = diag(1, 1, s)) and
+    free along z, settles where tau_zz = 0, i.e. where
+        r(s) = mu (s^2/g^2 - 1) + lambda ln(s / g^3) = 0,
+    and then carries tau_xx = mu (1 - s^2) / g^2.  Returns (s, tau_xx).
+    r is strictly increasing (r' = 2 mu s/g^2 + lambda/s > 0) with r(g) < 0
+    for g > 1, so Newton's method from the upper side converges monotonically;
+    a bracket keeps every iterate inside [lo, hi]."""
+    mu, lam = float(mat.mu), float(mat.lam)
+    g = float(g)
+    r = lambda s: mu * (s * s / (g * g) - 1.0) + lam * np.log(s / g ** 3)
+    dr = lambda s: 2.0 * mu * s / (g * g) + lam / s
+    lo, hi = 1e-6, max(g, 1.0)
+    while r(hi) < 0.0:
+        lo, hi = hi, 2.0 * hi
+    s = hi
+    for _ in range(100):
+        v = r(s)
+        if v > 0.0:
+            hi = s
+        else:
+            lo = s
+        step = s - v / dr(s)
+        s_new = step if lo < step < hi else 0.5 * (lo + hi)
+        if abs(s_new - s) <= 1e-15 * s:
+            s = s_new
+            break
+        s = s_new
+    return float(s), float(mu * (1.0 - s * s) / (g * g))

@@ -197,3 +197,20 @@ def test_confined_swell_gate():
     assert abs(lam - 2.0028) < 5e-5
     assert abs(tau(lam)[0, 0] - (-5147.403)) < 1e-3
     assert abs(tau(lam)[2, 2]) < 1e-9
+
+
+def test_confined_swell_helper_matches_the_model():
+    """constitutive.confined_swell_neohookean (the reference's closed-form
+    helper, constitutive.py:150-170): the reference's numbers at g = 1.5, and
+    at other materials and growths the oracle's neo-Hookean stress at the
+    returned stretch has tau_zz = 0 and the returned tau_xx."""
+    from morphompm_b200.config import Material
+    from morphompm_b200.constitutive import confined_swell_neohookean
+    s, txx = confined_swell_neohookean(Material(E=1e4, nu=0.3))
+    assert abs(s - 2.0028) < 5e-5 and abs(txx + 5147.403) < 1e-3
+    for E, nu, g in ((1e4, 0.3, 1.5), (2e3, 0.45, 1.2), (5e2, 0.2, 1.05), (1e4, 0.3, 1.0)):
+        mat = Material(E=E, nu=nu)
+        s, txx = confined_swell_neohookean(mat, g)
+        tau = O.stress(O.Model.elastic("nh", E, nu), np.diag([1.0, 1.0, s])[None], g * np.eye(3)[None])[0]
+        assert abs(tau[2, 2]) < 1e-9 * mat.mu
+        assert abs(tau[0, 0] - txx) < 1e-9 * mat.mu

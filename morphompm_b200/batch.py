@@ -154,8 +154,10 @@ class Batch:
         return self.n * self.n_steps
 
     def load(self, slab_host: np.ndarray, non_blocking=True):
-        """Copy a (24, n) host slab (pinned for async) into the device input."""
+        """Copy a (24, n) host slab (pinned for async) into the device input;
+        it replaces a prefetched input that no run has taken yet."""
         src = torch.from_numpy(slab_host) if isinstance(slab_host, np.ndarray) else slab_host
+        self._pending = False
         if self.order is None:
             self.slab0.copy_(src, non_blocking=non_blocking)
         else:

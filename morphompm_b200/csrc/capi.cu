@@ -434,7 +434,11 @@ int mpm_plan_create(const MpmScene* scenes, int32_t n_scenes, int32_t real_bytes
         pcur = sc.p_end;
         SceneAux a;
         a.cell_begin = cell;
-        a.ncells = (sc.shape[0] + 2) * (sc.shape[1] + 2) * (sc.shape[2] + 2);
+        // padded cells of the scene, in 64 bits: cell keys are 32-bit, so a
+        // scene (or batch) beyond 2^31 cells is refused rather than wrapped
+        const long long nc = (long long)(sc.shape[0] + 2) * (sc.shape[1] + 2) * (sc.shape[2] + 2);
+        if (nc >= (1LL << 31)) { delete P; return MPM_ERR_ARG; }
+        a.ncells = (int)nc;
         a.ntile[0] = (sc.shape[0] + T - 1) / T;
         a.ntile[1] = (sc.shape[1] + T - 1) / T;
         a.ntile[2] = (sc.shape[2] + TZ - 1) / TZ;
@@ -1045,7 +1049,9 @@ bool noalloc_layout(MpmPlan& P, const MpmScene& sc, int real_bytes, SceneAux& a)
     a.cell_begin = 0;
     a.tile_begin = 0;
     a.node_begin = 0;
-    a.ncells = (sc.shape[0] + 2) * (sc.shape[1] + 2) * (sc.shape[2] + 2);
+    const long long nc = (long long)(sc.shape[0] + 2) * (sc.shape[1] + 2) * (sc.shape[2] + 2);
+    if (nc >= (1LL << 31)) return false;     // beyond the 32-bit keys (and far beyond the scratch)
+    a.ncells = (int)nc;
     a.ntile[0] = (sc.shape[0] + T - 1) / T;
     a.ntile[1] = (sc.shape[1] + T - 1) / T;
     a.ntile[2] = (sc.shape[2] + TZ - 1) / TZ;

@@ -182,3 +182,35 @@ def test_budget_schedule_covers_the_engine_memory():
             if k > 1:                     # k = 1 is the floor, taken even when nothing fits
                 assert used <= budget + 8 * 256, (steps, frac, k, used, budget)
     lib.mpm_plan_destroy(h)
+
+
+def test_plan_refuses_grids_beyond_the_key_range():
+    """Cell keys are 32-bit: a scene or batch with 2^31 or more padded cells is
+    refused at plan creation (host only), not wrapped."""
+    lib = L.load()
+    h = C.c_void_p()
+    big = _scene(10, 0, (2048, 2048, 2048))          # 2050^3 padded cells
+    assert lib.mpm_plan_create((L.MpmScene * 1)(big), 1, 4, None, C.byref(h)) == L.MPM_ERR_ARG
+    ok = _scene(10, 0, (1000, 1000, 1000))           # 1002^3 < 2^31
+    assert lib.mpm_plan_create((L.MpmScene * 1)(ok), 1, 4, None, C.byref(h)) == L.MPM_OK
+    lib.mpm_plan_destroy(h)
+    three = (L.MpmScene * 3)(*(_scene(10, 10 * i, (1000, 1000, 1000)) for i in range(3)))
+    assert lib.mpm_plan_create(three, 3, 4, None, C.byref(h)) == L.MPM_ERR_ARG    # 3 x 1.006e9
+
+
+def test_noalloc_refuses_large_scenes_before_any_cuda_call():
+    """mpm_step_fwd_noalloc sizes its layout on the host first: a scene that
+    does not fit the fixed scratch, including one beyond the 32-bit cell keys,
+    returns MPM_ERR_TOO_LARGE without touching the device (the particle
+    pointers are never dereferenced on the host)."""
+    lib = L.load()
+    fake = L.MpmParticles()
+    fake.x, fake.v, fake.C, fake.F, fake.Fg = 4096, 8192, 12288, 16384, 20480
+    fake.sp3, fake.sc3, fake.sp9, fake.sc9 = 3, 1, 9, 1
+    out = L.MpmParticles()
+    out.x, out.v, out.C, out.F, out.Fg = 24576, 28672, 32768, 36864, 40960
+    out.sp3, out.sc3, out.sp9, out.sc9 = 3, 1, 9, 1
+    for shape in ((2048, 2048, 2048), (256, 256, 256)):
+        sc = _scene(10, 0, shape)
+        assert lib.mpm_step_fwd_noalloc(C.byref(sc), 4, C.byref(fake), C.byref(out), 1, 0, None, None) == \
+            L.MPM_ERR_TOO_LARGE

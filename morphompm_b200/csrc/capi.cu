@@ -952,6 +952,10 @@ int mpm_stress_vjp(const MpmScene* scene, int32_t real_bytes, int64_t n, const v
 
 int mpm_bin_keys(const MpmScene* scene, int32_t real_bytes, int64_t n, const void* x, int32_t* keys, void* stream) {
     if (!scene || n < 0 || !x || !keys || (real_bytes != 4 && real_bytes != 8)) return MPM_ERR_ARG;
+    // the keys are int32: the padded cells (and the "outside" key after them) must fit
+    if (!scene_ok(*scene) ||
+        (long long)(scene->shape[0] + 2) * (scene->shape[1] + 2) * (scene->shape[2] + 2) >= (1LL << 31))
+        return MPM_ERR_ARG;
     if (n == 0) return MPM_OK;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     int g = grid_for(n, 256);

@@ -214,3 +214,10 @@ def test_noalloc_refuses_large_scenes_before_any_cuda_call():
         sc = _scene(10, 0, shape)
         assert lib.mpm_step_fwd_noalloc(C.byref(sc), 4, C.byref(fake), C.byref(out), 1, 0, None, None) == \
             L.MPM_ERR_TOO_LARGE
+
+
+def test_bin_keys_refuses_grids_beyond_int32_keys():
+    lib = L.load()
+    sc = _scene(10, 0, (2048, 2048, 2048))
+    keys = (C.c_int32 * 10)()
+    assert lib.mpm_bin_keys(C.byref(sc), 8, 10, C.c_void_p(4096), keys, None) == L.MPM_ERR_ARG

@@ -121,7 +121,8 @@ int mpm_plan_workspace_bytes(const MpmPlan* plan, size_t* bytes);
 int mpm_plan_tape_bytes(const MpmPlan* plan, size_t* bytes);
 int64_t mpm_plan_num_particles(const MpmPlan* plan);
 /* Upload the scene table and index tables into the workspace and clear the
- * status word (stream-ordered; call once before the first step). */
+ * status word (stream-ordered; call once before the first step).  Binding
+ * again (another workspace) ends any chain of mpm_step_fwd_chain calls. */
 int mpm_plan_bind(MpmPlan* plan, void* workspace, void* stream);
 /* Copy the device status word into *status (synchronises the stream). */
 int mpm_plan_read_status(MpmPlan* plan, int32_t* status, void* stream);

@@ -577,6 +577,9 @@ int mpm_plan_bind(MpmPlan* P, void* workspace, void* stream) {
     if (!P || !workspace || (reinterpret_cast<uintptr_t>(workspace) % ALIGN) != 0) return MPM_ERR_ARG;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     P->ws = static_cast<char*>(workspace);
+    // a new workspace holds no emitted keys, records or tile flags: end any chain
+    P->chain_valid = false;
+    P->tile_flags_pending = false;
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return MPM_ERR_CUDA;
     cudaDeviceGetAttribute(&P->n_sm, cudaDevAttrMultiProcessorCount, dev);

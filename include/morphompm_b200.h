@@ -179,7 +179,8 @@ int mpm_plan_set_particle_mass(MpmPlan* plan, const void* mass, const void* vol0
 /* Optional per-particle growth field phi_p (growth_mode 1), real type: the
  * field growth law g_p(t) = 1 + A ramp(t) phi_p of the reference's growth
  * drivers (docs/PHASE3_morphogenesis.md:55-57), evaluated on the device; the
- * reference's own driver sets Fg = g I per call (integrate.py:31-34). */
+ * reference's own driver sets Fg = g I per call (integrate.py:31-34).
+ * Ends any chain of mpm_step_fwd_chain calls. */
 int mpm_plan_set_growth_field(MpmPlan* plan, const void* phi);
 
 /* One forward MLS-MPM step for every scene of the batch:

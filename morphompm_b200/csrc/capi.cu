@@ -654,6 +654,7 @@ int mpm_plan_set_particle_mass(MpmPlan* P, const void* mass, const void* vol0) {
 int mpm_plan_set_growth_field(MpmPlan* P, const void* phi) {
     if (!P) return MPM_ERR_ARG;
     P->phi = phi;
+    P->chain_valid = false;     // records formed with the old growth field
     return MPM_OK;
 }
 

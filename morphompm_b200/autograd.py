@@ -109,6 +109,8 @@ def rollout_loss(x0, growth, model, cfg, n_steps: int, advect: bool = True, loss
     """Loss of the final state of an n_steps trajectory from the rest state at
     x0 (n, 3) with Fg = growth I (0-d tensor) or growth (n, 3, 3); the same
     functional as ``integrate.dloss_dg``, differentiable in x0 and growth."""
+    from .integrate import check_loss
+    check_loss(loss, x_obs)
     if not isinstance(growth, torch.Tensor):
         growth = torch.tensor(float(growth), dtype=x0.dtype, device=x0.device)
     if ckpt_every is None:

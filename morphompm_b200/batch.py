@@ -79,6 +79,8 @@ class Batch:
         reorder: store each scene's particles in the cell order of their
         initial positions (layout.py); inputs and the state accessors keep the
         caller's particle order."""
+        from .integrate import check_loss
+        check_loss(loss, x_obs)
         self.scenes = [dict(s) for s in scenes]   # set_params edits these copies
         self.n_steps = n_steps
         self.dtype = dtype

@@ -92,12 +92,23 @@ def _slab_from_points(pts_dev: torch.Tensor) -> torch.Tensor:
     return slab
 
 
+def check_loss(loss: str, x_obs) -> None:
+    """The trajectory losses: "detF" (sum det F of the final state, the
+    reference's, integrate.py:41-52) and "mse" (mean squared distance of the
+    final positions to x_obs, which it needs)."""
+    if loss not in ("detF", "mse"):
+        raise ValueError(f"loss must be 'detF' or 'mse', not {loss!r}")
+    if loss == "mse" and x_obs is None:
+        raise ValueError("loss='mse' needs x_obs, the observed final positions (n, 3)")
+
+
 def dloss_dg(pts, model, cfg, g, n_steps, advect, loss: str = "detF", x_obs=None,
              ckpt_every: Optional[int] = None):
     """d(loss of the final state)/dg for Fg = g I (integrate.py:45-52).
     loss="detF": sum det F_final (the reference's); loss="mse": mean
     |x_final - x_obs|^2."""
     from .trajectory import Rollout
+    check_loss(loss, x_obs)
     if is_external(model):
         return _dloss_dg_steps(pts, model, cfg, g, n_steps, advect, loss, x_obs)
     if ckpt_every is None:
@@ -172,6 +183,7 @@ def dloss_dparams(pts, model, cfg, g, n_steps, advect, loss: str = "detF", x_obs
     no counterpart in the reference (its VJPs stop at F, Fg and C); they come
     from mpm_step_bwd_params.  Elastic models only (mu, lambda of the model)."""
     from .trajectory import Rollout
+    check_loss(loss, x_obs)
     if is_external(model):
         raise TypeError("material-parameter gradients need a built-in elastic model (mu, lambda)")
     if ckpt_every is None:

@@ -18,3 +18,17 @@ def test_misshaped_state_is_refused(field, shape):
     st[field] = np.zeros(shape)
     with pytest.raises(ValueError, match=field):
         transfer.step(ParticleState(**st), NeoHookean(Material()), SimConfig())
+
+
+@pytest.mark.parametrize("loss,x_obs", [("l2", None), ("mse", None)])
+def test_trajectory_losses_are_checked_before_device_work(loss, x_obs):
+    from morphompm_b200 import integrate
+    from morphompm_b200.batch import Batch
+    from morphompm_b200 import scenes
+    pts = np.random.default_rng(0).uniform(0.3, 0.6, size=(10, 3))
+    with pytest.raises(ValueError, match="loss"):
+        integrate.dloss_dg(pts, NeoHookean(Material()), SimConfig(), 1.1, 2, True, loss=loss, x_obs=x_obs)
+    with pytest.raises(ValueError, match="loss"):
+        integrate.dloss_dparams(pts, NeoHookean(Material()), SimConfig(), 1.1, 2, True, loss=loss, x_obs=x_obs)
+    with pytest.raises(ValueError, match="loss"):
+        Batch(scenes.config4(n_scenes=2, n_lo=100, n_hi=200), 2, loss=loss, x_obs=x_obs)

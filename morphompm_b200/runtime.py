@@ -105,7 +105,11 @@ def tuning_struct(t: Optional[dict]) -> L.MpmTuning:
 
 
 class Plan:
-    """A bound batch plan: scene table + workspace on the current CUDA device."""
+    """A bound batch plan: scene table + workspace on one CUDA device
+    (``device``, default the current one).  The library launches on the
+    current device, so every later call on the plan must run with that device
+    current (one process per GPU, as torchrun launches them, satisfies this);
+    ``stream=None`` means the current stream of the current device."""
 
     def __init__(self, scenes: List[SceneSpec], dtype=torch.float64, tuning: Optional[dict] = None,
                  device=None, stream=None):

@@ -7,8 +7,10 @@ graph-captured launch sequence per trajectory).
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 One bench step = one forward + loss + adjoint trajectory over the whole batch.
-Prints one JSON line (rank 0).  Under torchrun every rank runs its own batch
-(different seed; no data-path collective): weak scaling, time = max over ranks.
+Prints one JSON line (rank 0).  Under torchrun the batch has 256 x ranks scenes
+(one seed), LPT-sharded over the ranks by particles x steps, so every rank holds
+about the 1-GPU work (weak scaling); no data-path collective; time = max over
+ranks; per-scene results are gathered to every rank in scene order afterwards.
 """
 from __future__ import annotations
 
@@ -276,7 +278,13 @@ def main():
     from morphompm_b200.batch import Batch, host_slab, load_tuned
     from morphompm_b200.trajectory import sqrt_schedule
 
-    scn = S.config4(seed=4 + 1000 * rank, n_scenes=a.scenes)
+    # one fixed batch of scenes x ranks scenes (seed 4; its first 256 scenes are
+    # the 1-GPU workload), LPT-sharded over the ranks by particles x steps:
+    # every rank holds about the same work (weak scaling), no data-path collective
+    from morphompm_b200.shard import lpt_assign, gather_scenes, fixed_order_sum
+    scn_all = S.config4(seed=4, n_scenes=a.scenes * world)
+    mine = lpt_assign([s["x"].shape[0] * a.mpm_steps for s in scn_all], world)[rank]
+    scn = [scn_all[i] for i in mine]
     n_tot = sum(s["x"].shape[0] for s in scn)
     ck = a.ckpt_every if a.ckpt_every in ("auto", "sqrt") else int(a.ckpt_every)
     tuning = load_tuned(scn, torch.float32) or {}
@@ -306,6 +314,7 @@ def main():
     for _ in range(a.warmup):
         b.replay()
     torch.cuda.synchronize()
+    fb0 = plan.fp64_fallbacks()      # cumulative device counter: read its change over the timed replays
     if world > 1:
         dist.barrier()
     clocks = ClockSampler(dev.index if dev.index is not None else 0)
@@ -320,11 +329,12 @@ def main():
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
     clk = clocks.stop()
+    fallbacks = (plan.fp64_fallbacks() - fb0) / a.steps
     prof = plan.profile_end()
     from morphompm_b200.shard import max_over_ranks, sum_over_ranks
     ms = max_over_ranks(ms, dev)
     ms_per = ms / a.steps
-    # every rank runs a batch of its own (its own seed): the job's particles are the sum
+    # the job's particles: the sum over the ranks' shards
     n_all = int(sum_over_ranks(n_tot, dev))
     units = n_all * a.mpm_steps
     value = units / (ms_per / 1e3)
@@ -350,6 +360,11 @@ def main():
     e2e = {"value": units / (ms_e2e / a.steps / 1e3), "unit": UNIT,
            "h2d_bytes_per_step": int(slab_h.numel() * slab_h.element_size()),
            "d2h_bytes_per_step": int(2 * 8 * len(scn))}
+    # every scene's loss and d loss / d g in scene order on every rank, and the
+    # gradient of a growth amplitude shared by all scenes (fixed-order sum)
+    full = gather_scenes(np.stack([loss_h.numpy(), grad_h.numpy()], 1), mine, len(scn_all), dev)
+    gathered = {"scenes": len(scn_all), "loss_sum": fixed_order_sum(full[:, 0]),
+                "shared_growth_grad": fixed_order_sum(full[:, 1])}
 
     # roofline of the dominant kernel (HBM bound: no dense contraction here)
     tot_ms, nl = prof.get(dominant, (float("nan"), 0))
@@ -377,25 +392,31 @@ def main():
     step_bytes = w * (156 + 32 * 0.2) * n_tot * a.mpm_steps
     step_roof = {"bytes_per_particle_step": w * (156 + 32 * 0.2), "achieved_gbs": step_bytes / (ms_per / 1e3) / 1e9,
                  "frac": step_bytes / (ms_per / 1e3) / 1e9 / peak}
-    fallbacks = plan.fp64_fallbacks()
     status = plan.status()
+    # every Hencky particle is evaluated once per forward step and once per
+    # reverse step (store-all schedule; recompute adds forward evaluations)
+    n_hencky = sum(int(sc["x"].shape[0]) for sc in scn if sc["model"] == "hencky")
+    recomputed = a.mpm_steps - a.mpm_steps // max(1, k) if k < a.mpm_steps else 0
+    hencky_evals = n_hencky * (2 * a.mpm_steps + recomputed)
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
             "ms_per_step": ms_per, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "scenes": len(scn), "particles": n_all,
+            "config": {"workload": WORKLOAD, "scenes": len(scn_all), "particles": n_all,
                        "mpm_steps": a.mpm_steps, "ckpt_every": k, "l2": "inputs larger than L2 "
                        f"({n_tot * 24 * 4 / 1e6:.0f} MB state per GPU)", "schedule": plan.tuning or "defaults",
-                       "parallelism": f"{world} independent batches (no collective)"},
+                       "parallelism": f"{world} rank(s), one {len(scn_all)}-scene batch LPT-sharded by "
+                                      "particles x steps (no data-path collective)"},
             "roofline": roof, "step_roofline": step_roof, "e2e": e2e,
             "gpu_launches": int(launches_per_traj * a.steps), "clocks": clk,
             "kernel_ms_per_trajectory": {kk: round(v[0], 3) for kk, v in prof_all.items()},
-            "fp64_hencky_fallbacks_per_trajectory": None, "device_status": status,
-            "active_tile_cap": plan.tuning.get("active_tile_cap")}
-    line["fp64_hencky_fallbacks_per_trajectory"] = fallbacks / max(1, a.warmup + a.steps + 3)
+            "fp64_hencky_fallbacks_per_trajectory": fallbacks,
+            "fp64_hencky_fallback_fraction": fallbacks / max(1, hencky_evals),
+            "device_status": status, "active_tile_cap": plan.tuning.get("active_tile_cap"),
+            "gathered": gathered}
 
     if rank == 0 and not a.no_plain:
-        line["fp64_plain"] = plain_leg(scn, a, value, tuning)
+        line["fp64_plain"] = plain_leg(scn, a, value, peak, tuning)
     if rank == 0 and not a.no_cpu:
         line["cpu_baseline"] = cpu_baseline(scn, a.cpu_seconds)
         line["cpu_reference_forward"] = cpp_reference_forward()
@@ -502,16 +523,21 @@ def run_other(a):
     print(json.dumps(line), flush=True)
 
 
-def plain_leg(scn, a, value32, tuning32=None):
+def plain_leg(scn, a, value32, peak, tuning32=None):
     """FP64 plain path: one scene at a time, eager launches per step (the
     drop-in transfer path), same trajectory.  Timed on a sample of scenes
-    spread over the size range; FP32 error vs FP64 on the same scenes."""
+    spread over the size range, with the throughput and the FP32-batched ratio
+    of each sampled scene, the HBM roofline of the plain path (1299.2 B per
+    particle-step in FP64), and the FP32 error vs FP64 on the same scenes.
+    The whole batch in FP64, graph-captured, separates the gain of batching
+    from the gain of FP32."""
     import torch
     from morphompm_b200.batch import Batch, host_slab
     idx = sorted(range(len(scn)), key=lambda i: scn[i]["x"].shape[0])
     sample = [idx[int(round(q * (len(idx) - 1)))] for q in np.linspace(0.0, 1.0, 6)]
     units, secs = 0, 0.0
     errs = {"F": 0.0, "x": 0.0, "dLdg_rel": 0.0}
+    per_scene = []
     for i in sample:
         s = scn[i]
         b64 = Batch([s], a.mpm_steps, dtype=torch.float64, ckpt_every="auto")
@@ -521,8 +547,13 @@ def plain_leg(scn, a, value32, tuning32=None):
         t0 = time.perf_counter()
         b64.run()
         torch.cuda.synchronize()
-        secs += time.perf_counter() - t0
-        units += s["x"].shape[0] * a.mpm_steps
+        dt = time.perf_counter() - t0
+        secs += dt
+        n_i = s["x"].shape[0]
+        units += n_i * a.mpm_steps
+        v_i = n_i * a.mpm_steps / dt
+        per_scene.append({"particles": n_i, "grid": int(s["shape"][0]), "model": s["model"], "value": v_i,
+                          "ms_per_mpm_step": dt * 1e3 / a.mpm_steps, "fp32_batched_over_this": value32 / v_i})
         b32 = Batch([s], a.mpm_steps, dtype=torch.float32, ckpt_every="auto", tuning=tuning32)
         b32.load(host_slab([s], np.float32), non_blocking=False)
         b32.run()
@@ -533,9 +564,26 @@ def plain_leg(scn, a, value32, tuning32=None):
         errs["x"] = max(errs["x"], float(np.max(np.abs(f64[0:3] - f32[0:3]))))
         g64, g32 = float(b64.dloss_dg[0]), float(b32.dloss_dg[0])
         errs["dLdg_rel"] = max(errs["dLdg_rel"], abs(g64 - g32) / max(abs(g64), 1e-300))
+        del b64, b32
     v64 = units / secs
+    bpp = 8 * (156 + 32 * 0.2)
+    torch.cuda.empty_cache()
+    # the whole batch in FP64, graph-captured (batching without the FP32 gain)
+    bb = Batch(scn, a.mpm_steps, dtype=torch.float64, ckpt_every="auto", tuning=None)
+    bb.load(host_slab(scn, np.float64), non_blocking=False)
+    ms_b = _timed_trajectories(bb, 2, 1)
+    n_all = sum(s["x"].shape[0] for s in scn)
+    v64b = n_all * a.mpm_steps / (ms_b / 1e3)
+    del bb
+    torch.cuda.empty_cache()
     return {"value": v64, "unit": UNIT, "sample": f"{len(sample)} scenes spread over the size range, "
             f"{a.mpm_steps} steps fwd+adj each, eager launches, FP64", "fp32_batched_over_fp64_plain": value32 / v64,
+            "per_scene": per_scene,
+            "roofline": {"bound": "hbm", "bytes_per_particle_step": bpp, "achieved": v64 * bpp / 1e9, "peak": peak,
+                         "unit": "GB/s", "frac": v64 * bpp / 1e9 / peak},
+            "fp64_batched": {"value": v64b, "ms_per_trajectory": ms_b,
+                             "roofline_frac": v64b * bpp / 1e9 / peak,
+                             "batching_gain": v64b / v64, "fp32_gain": value32 / v64b},
             "fp32_error_vs_fp64": errs}
 
 

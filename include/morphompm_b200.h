@@ -309,7 +309,9 @@ int mpm_loss_mse(MpmPlan* plan, const void* x, int64_t sp3, int64_t sc3, const v
  *   - scene->p_begin must be 0; scene->p_end is the particle count.
  *   - The first call on a device looks the array up (cudaGetSymbolAddress)
  *     with that device current; make that first call before any stream
- *     capture.
+ *     capture.  The address belongs to the device's context: after a device
+ *     reset (cudaDeviceReset) the next call looks it up again, so that call
+ *     too must come before any stream capture.
  *   - All calls share the one array: calls whose GPU work overlaps (two
  *     streams, two host threads) race and must be serialised by the caller.
  *     Each call clears the parts that must start at zero.

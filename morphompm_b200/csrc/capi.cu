@@ -1,6 +1,7 @@
 // Host side of the C ABI (include/morphompm_b200.h): plan construction,
 // workspace/tape layout, and the launch sequences of one forward and one
 // reverse growth step.  No device memory is allocated here.
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <nvtx3/nvToolsExt.h>
 
@@ -8,6 +9,7 @@
 #include <atomic>
 #include <climits>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <vector>
 
@@ -224,6 +226,19 @@ int launch_nodes(MpmPlan* P, int mode, const Ctx& ctx, const int* active, const 
     return cudaLaunchKernel(f2, dim3(ctas), dim3(1024), a2, 0, st) == cudaSuccess ? MPM_OK : MPM_ERR_CUDA;
 }
 
+// P2G phase 1 from records staged in shared memory (schedule scatter_oxb = -1):
+// one warp per STAGE_CPW occupied cells, a persistent grid of CTAs
+template <typename R, int MODE>
+void launch_staged(MpmPlan* P, const Ctx& ctx, const unsigned* perm, const R* payload, const MpmParticles& in,
+                   const MpmCotangents& ob, int advect, cudaStream_t st) {
+    R* S = at<R>(P, P->o_sums);
+    const long long cap = P->n;
+    const long long chunks = (P->n + STAGE_CPW - 1) / STAGE_CPW;      // an upper bound of the cell chunks
+    const long long want = (chunks + STAGE_WARPS - 1) / STAGE_WARPS;
+    const int blocks = (int)std::max<long long>(1, std::min<long long>(want, (long long)P->n_sm * 16));
+    cell_sums_staged_kernel<R, MODE><<<blocks, 32 * STAGE_WARPS, 0, st>>>(ctx, perm, payload, in, ob, S, cap, advect);
+}
+
 // two-phase P2G: per-cell stencil sums, then per-node gather + grid epilogue
 template <typename R>
 int launch_p2g(MpmPlan* P, int mode, const Ctx& ctx, const unsigned* perm, const R* payload, const int* active,
@@ -233,9 +248,13 @@ int launch_p2g(MpmPlan* P, int mode, const Ctx& ctx, const unsigned* perm, const
     long long cap = P->n;
     int blocks1 = (int)std::min<long long>((P->n + 127) / 128, (long long)P->n_sm * 16);
     blocks1 = std::max(1, blocks1);
-    void* f1 = mode == 0 ? sums_fn<R, 0>(P->tune.scatter_oxb) : sums_fn<R, 1>(P->tune.scatter_oxb);
-    void* a1[] = {(void*)&ctx, (void*)&perm, (void*)&payload, (void*)&S, (void*)&cap};
-    if (cudaLaunchKernel(f1, dim3(blocks1), dim3(128), a1, 0, st) != cudaSuccess) return MPM_ERR_CUDA;
+    if (mode == 0 && P->tune.scatter_oxb == -1) {
+        launch_staged<R, 0>(P, ctx, perm, payload, MpmParticles{}, MpmCotangents{}, advect, st);
+    } else {
+        void* f1 = mode == 0 ? sums_fn<R, 0>(P->tune.scatter_oxb) : sums_fn<R, 1>(P->tune.scatter_oxb);
+        void* a1[] = {(void*)&ctx, (void*)&perm, (void*)&payload, (void*)&S, (void*)&cap};
+        if (cudaLaunchKernel(f1, dim3(blocks1), dim3(128), a1, 0, st) != cudaSuccess) return MPM_ERR_CUDA;
+    }
     P->launches += 1;   // the Site around this call counts one
     return launch_nodes<R>(P, mode, ctx, active, nact, grid_out, grid_fwd, advect, st);
 }
@@ -331,7 +350,9 @@ int step_bwd_R(MpmPlan* P, const MpmParticles& in, const void* outC, const MpmCo
         long long cap = P->n;
         int blocks1 = (int)std::min<long long>((P->n + 127) / 128, (long long)P->n_sm * 16);
         blocks1 = std::max(1, blocks1);
-        if (P->tune.scatter_oxb == 3 && sizeof(R) == 4)
+        if (P->tune.scatter_oxb == -1)
+            launch_staged<R, 1>(P, ctx, tp.perm, nullptr, in, ob, advect, st);
+        else if (P->tune.scatter_oxb == 3 && sizeof(R) == 4)
             cell_sums_adj_kernel<R, 3><<<blocks1, 128, 0, st>>>(ctx, tp.perm, in, ob, S, cap, advect);
         else
             cell_sums_adj_kernel<R, 1><<<blocks1, 128, 0, st>>>(ctx, tp.perm, in, ob, S, cap, advect);
@@ -420,8 +441,9 @@ int mpm_plan_create(const MpmScene* scenes, int32_t n_scenes, int32_t real_bytes
     if (P->tune.tile_xy != 8 && P->tune.tile_xy != 16) P->tune.tile_xy = 4;
     if (P->tune.tile_z != 8 && P->tune.tile_z != 16) P->tune.tile_z = 4;
     if (P->tune.scatter_ctas_per_sm <= 0) P->tune.scatter_ctas_per_sm = 1;
-    if (P->tune.scatter_oxb != 1 && P->tune.scatter_oxb != 3) P->tune.scatter_oxb = real_bytes == 4 ? 3 : 1;
-    if (real_bytes == 8) P->tune.scatter_oxb = 1;
+    if (P->tune.scatter_oxb != -1 && P->tune.scatter_oxb != 1 && P->tune.scatter_oxb != 3)
+        P->tune.scatter_oxb = real_bytes == 4 ? 3 : 1;
+    if (real_bytes == 8 && P->tune.scatter_oxb == 3) P->tune.scatter_oxb = 1;
     // the per-particle kernels are compiled for at most 256 threads per block
     if (P->tune.particle_block != 64 && P->tune.particle_block != 128) P->tune.particle_block = 256;
     if (P->tune.fp64_gap_thresh == 0.0f) P->tune.fp64_gap_thresh = 1e-6f;
@@ -1017,28 +1039,68 @@ __device__ __align__(256) unsigned char g_noalloc_scratch[MPM_NOALLOC_SCRATCH_BY
 
 constexpr int NOALLOC_MAX_DEVICES = 64;
 struct NoallocDevice {
-    std::atomic<void*> ptr{nullptr};
-    std::atomic<int> n_sm{0};
+    std::mutex mu;
+    unsigned long long ctx_id = 0;   // driver id of the context the address belongs to (0: none yet)
+    void* ptr = nullptr;
+    int n_sm = 0;
 };
 NoallocDevice g_noalloc_dev[NOALLOC_MAX_DEVICES];
 
-// Device address of the scratch array on the current device (looked up once
-// per device, with that device current).
+// Unique id of the calling thread's current driver context (0 when none is
+// current yet).  A device reset destroys the context and the module loaded in
+// it; the next context has a new id, so the scratch address is looked up
+// again.  The two driver calls are fetched through the runtime once, so the
+// library does not link the driver library itself.
+typedef CUresult (*CtxGetCurrentFn)(CUcontext*);
+typedef CUresult (*CtxGetIdFn)(CUcontext, unsigned long long*);
+int current_context_id(unsigned long long* id) {
+    static CtxGetCurrentFn get_current = nullptr;
+    static CtxGetIdFn get_id = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &f, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_current = reinterpret_cast<CtxGetCurrentFn>(f);
+        f = nullptr;
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetId", &f, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_id = reinterpret_cast<CtxGetIdFn>(f);
+    });
+    if (!get_current || !get_id) return MPM_ERR_CUDA;
+    CUcontext c = nullptr;
+    *id = 0;
+    if (get_current(&c) != CUDA_SUCCESS) return MPM_ERR_CUDA;
+    if (c && get_id(c, id) != CUDA_SUCCESS) return MPM_ERR_CUDA;
+    return MPM_OK;
+}
+
+// Device address of the scratch array in the current device's context.  The
+// lookup (cudaGetSymbolAddress) runs with that device current, once per
+// context: on the first call on a device, and again on the first call after a
+// device reset.
 int noalloc_scratch(void** out, int* n_sm) {
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return MPM_ERR_CUDA;
     if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) return MPM_ERR_UNSUPPORTED;
     NoallocDevice& d = g_noalloc_dev[dev];
-    void* p = d.ptr.load();
-    if (!p) {
+    std::lock_guard<std::mutex> lock(d.mu);
+    unsigned long long id = 0;
+    if (current_context_id(&id)) return MPM_ERR_CUDA;
+    if (id == 0 || id != d.ctx_id || !d.ptr) {
+        void* p = nullptr;
+        // creates the device's context when none is current yet
         if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return MPM_ERR_CUDA;
         int sm = 0;
         if (cudaDeviceGetAttribute(&sm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return MPM_ERR_CUDA;
-        d.n_sm.store(sm);
-        d.ptr.store(p);
+        if (current_context_id(&id) || id == 0) return MPM_ERR_CUDA;
+        d.ptr = p;
+        d.n_sm = sm;
+        d.ctx_id = id;
     }
-    *out = p;
-    *n_sm = d.n_sm.load();
+    *out = d.ptr;
+    *n_sm = d.n_sm;
     return MPM_OK;
 }
 

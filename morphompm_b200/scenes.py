@@ -63,16 +63,18 @@ def config1(seed=1):
                 growth_A=0.1, ramp_steps=100, phi=None, wall=2, steps=100)
 
 
-def config2(seed=2):
+def config2(seed=2, length=64, steps=2000):
+    """Bilayer strip of `length` x 8 x 8 cells from x-cell 16 (64 for the full
+    workload), top half growing to g = 1.2 over `steps` steps, clamped end."""
     dx = 1.0 / 32
     rng = np.random.default_rng(seed)
-    x = stratified_cells(rng, (16, 12, 12), (80, 20, 20), dx)
+    x = stratified_cells(rng, (16, 12, 12), (16 + length, 20, 20), dx)
     mu, lam = _elastic(1e3, 0.3)
     phi = (x[:, 1] >= 0.5).astype(np.float64)      # top layer grows
-    return dict(name="bilayer strip 96x32x32, 32768 particles", x=x, shape=(96, 32, 32), dx=dx,
+    return dict(name=f"bilayer strip 96x32x32, {x.shape[0]} particles", x=x, shape=(96, 32, 32), dx=dx,
                 dt=5e-5, damping=0.05, density=1.0, model="hencky", E=1e3, nu=0.3, mu=mu, lam=lam,
-                growth_A=0.2, ramp_steps=2000, phi=phi, wall=0,
-                clamp_lo=(0, 0, 0), clamp_hi=(18, 32, 32), steps=2000)
+                growth_A=0.2, ramp_steps=steps, phi=phi, wall=0,
+                clamp_lo=(0, 0, 0), clamp_hi=(18, 32, 32), steps=steps)
 
 
 def config3(seed=3):
@@ -109,7 +111,9 @@ def config4(seed=4, n_scenes=256, n_lo=2048, n_hi=65536):
     return out
 
 
-def config5(seed=5, cells=(128, 128, 16), edge=256):
+def config5(seed=5, cells=(128, 128, 16), edge=256, steps=1000):
+    """Herschel-Bulkley sheet of `cells` cells centred in an edge^3 grid with
+    the radial growth field g(r) = 1 + 0.2 exp(-r^2 / 0.05)."""
     dx = 1.0 / edge
     rng = np.random.default_rng(seed)
     lo = [(edge - c) // 2 for c in cells]
@@ -117,7 +121,7 @@ def config5(seed=5, cells=(128, 128, 16), edge=256):
     x = stratified_cells(rng, lo, hi, dx)
     r2 = (x[:, 0] - 0.5) ** 2 + (x[:, 1] - 0.5) ** 2
     phi = np.exp(-r2 / 0.05)
-    return dict(name="HB sheet 256^3, 2M particles", x=x, shape=(edge, edge, edge), dx=dx,
+    return dict(name=f"HB sheet {edge}^3, {x.shape[0]} particles", x=x, shape=(edge, edge, edge), dx=dx,
                 dt=1e-5, damping=0.05, density=1.0, model="hb",
                 hb=dict(kappa=1e4, K=1.0, n=0.5, tau_y=10.0, m=100.0, eps=1e-4),
-                growth_A=0.2, ramp_steps=0, phi=phi, wall=2, steps=1000)
+                growth_A=0.2, ramp_steps=0, phi=phi, wall=2, steps=steps)

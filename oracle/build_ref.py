@@ -15,6 +15,14 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT = os.path.join(HERE, "_ref", "libgrowth_ref.so")
+# Where this recipe reads the reference sources in the build container; the
+# MORPHOMPM_REF environment variable or --ref points it elsewhere.
+REF_MOUNT = "/root/reference"
+
+
+def ref_root() -> str:
+    """Root of the reference project: MORPHOMPM_REF, else the build container's mount."""
+    return os.environ.get("MORPHOMPM_REF") or REF_MOUNT
 
 
 def build(ref_root: str, quiet: bool = False) -> str | None:
@@ -32,9 +40,9 @@ def build(ref_root: str, quiet: bool = False) -> str | None:
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default=os.environ.get("MORPHOMPM_REF", "/root/reference"))
+    ap.add_argument("--ref", default=None, help="reference root (default: MORPHOMPM_REF, else the build mount)")
     a = ap.parse_args()
-    out = build(a.ref)
+    out = build(a.ref or ref_root())
     if out:
         print(out)
 

@@ -1,7 +1,7 @@
 """Generate the golden fixtures in this folder by running the UNMODIFIED reference
 package (2nugu/morphompm, ``python/morphompm``) read-only.
 
-    python tests/golden/make_golden.py [--ref /path/to/reference]
+    python tests/golden/make_golden.py --ref /path/to/reference [--only io|c1full]
 
 The reference cannot travel to the GPU machine, so its outputs are committed as
 small ``.npz`` fixtures.  Every fixture records the exact inputs it was made from.
@@ -185,6 +185,44 @@ def make_c1_head(ref):
                         x=st.x, F=st.F, v=st.v)
 
 
+def make_c1_full(ref):
+    """The whole 100-step free-swell cube of ``make_c1_head`` through the
+    reference step, then its trajectory adjoint through the reference
+    ``step_vjp`` for the loss sum det F (integrate.py:45-52).  The caller
+    re-sets Fg = g(t) I before every step, so each step's Fg is an input of
+    its own: its cotangent does not flow back into the previous step, and
+    d loss / d A = sum_t ramp(t) sum_p tr(Fg_bar_t).  Takes about 15 minutes
+    on one core."""
+    config, constitutive, transfer, integrate, diff, state = ref
+    sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+    from morphompm_b200 import scenes
+    sc = scenes.config1()
+    cfg = config.SimConfig(N=32, dx=sc["dx"], dt=sc["dt"], damping=sc["damping"], sp=sc["dx"] / 2,
+                           material=config.Material(E=1e3, nu=0.3, density=1.0))
+    model = constitutive.NeoHookean(cfg.material)
+    st = state.ParticleState.rest(sc["x"])
+    steps = sc["steps"]
+    caches, ramps = [], []
+    for t in range(steps):
+        r = min(1.0, (t + 1) / sc["ramp_steps"])
+        st.Fg[:] = (1.0 + sc["growth_A"] * r) * np.eye(3)
+        st, cache = transfer.step(st, model, cfg, advect=True)
+        caches.append(cache)
+        ramps.append(r)
+    n = st.n
+    loss = integrate.loss_detF(st.F)
+    xb, vb = np.zeros((n, 3)), np.zeros((n, 3))
+    Cb = np.zeros((n, 3, 3))
+    Fb = np.stack([np.linalg.det(st.F[p]) * np.linalg.inv(st.F[p]).T for p in range(n)])
+    dA = 0.0
+    for t in reversed(range(steps)):
+        xb, vb, Cb, Fb, Fgb = transfer.step_vjp(caches[t], xb, vb, Cb, Fb, np.zeros((n, 3, 3)), advect=True)
+        dA += ramps[t] * integrate.iso_growth_grad(Fgb)
+        caches[t] = None
+    np.savez_compressed(os.path.join(HERE, "c1_full.npz"), steps=steps, x=st.x, F=st.F, loss=loss,
+                        dloss_dA=dA, x0_bar=xb, F0_bar=Fb)
+
+
 def make_io(ref_root):
     """Files written by the reference's own I/O adapters (io.py:29-111) for a
     small state and config, so that the device-side writers are checked byte
@@ -210,20 +248,28 @@ def make_io(ref_root):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default=os.environ.get("MORPHOMPM_REF", "/root/reference"))
+    ap.add_argument("--ref", default=os.environ.get("MORPHOMPM_REF"),
+                    help="root of the reference project (or set MORPHOMPM_REF)")
     ap.add_argument("--skip-c1", action="store_true")
-    ap.add_argument("--only", choices=["io"], default=None, help="write one group of fixtures")
+    ap.add_argument("--only", choices=["io", "c1full"], default=None, help="write one group of fixtures")
     a = ap.parse_args()
+    if not a.ref:
+        ap.error("the reference root is required: --ref PATH or MORPHOMPM_REF")
     if a.only == "io":
         make_io(a.ref)
         print("golden I/O fixtures written to", HERE)
         return
     ref = _import_ref(a.ref)
+    if a.only == "c1full":
+        make_c1_full(ref)
+        print("golden c1_full fixture written to", HERE)
+        return
     make_constitutive(ref)
     make_step(ref)
     make_gates(ref)
     if not a.skip_c1:
         make_c1_head(ref)
+        make_c1_full(ref)
     make_io(a.ref)
     print("golden fixtures written to", HERE)
 

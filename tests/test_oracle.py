@@ -8,8 +8,9 @@ import numpy as np
 import pytest
 
 from oracle import mpm_oracle as O
+from oracle.build_ref import ref_root
 
-REF = os.environ.get("MORPHOMPM_REF", "/root/reference")
+REF = ref_root()
 
 
 def rel(a, b):
@@ -98,6 +99,28 @@ def test_c1_head(golden):
     st, _ = O.rollout(O.State.rest(c["x"]), m, sc, int(d["steps"]), advect=True, growth=gr, keep_caches=False)
     assert rel(st.F, d["F"]) < 1e-12
     assert rel(st.x, d["x"]) < 1e-14
+
+
+def test_c1_full_length_and_adjoint(golden):
+    """The whole 100-step config-1 trajectory and its adjoint (sum det F, d/dA
+    of the growth ramp) against the reference's own run of them."""
+    from morphompm_b200 import scenes
+    d = golden("c1_full.npz")
+    c = scenes.config1()
+    sc = O.Scene(shape=(32, 32, 32), dx=c["dx"], dt=c["dt"], damping=c["damping"],
+                 pmass=c["density"] * (c["dx"] / 2) ** 3, vol0=(c["dx"] / 2) ** 3)
+    gr = O.Growth(A=c["growth_A"], ramp_steps=c["ramp_steps"])
+    st, caches = O.rollout(O.State.rest(c["x"]), O.Model.elastic("nh", c["E"], c["nu"]), sc, int(d["steps"]),
+                           advect=True, growth=gr)
+    assert np.max(np.abs(st.F - d["F"])) < 1e-12
+    assert np.max(np.abs(st.x - d["x"])) < 1e-13
+    assert abs(O.loss_detF(st.F) - float(d["loss"])) < 1e-12 * float(d["loss"])
+    n = c["x"].shape[0]
+    z3, z33 = np.zeros((n, 3)), np.zeros((n, 3, 3))
+    xb, _, _, Fb, _, dA = O.rollout_vjp(caches, z3, z3, z33, O.seed_detF(st.F), z33, advect=True, growth=gr)
+    assert abs(dA - float(d["dloss_dA"])) < 1e-11 * abs(float(d["dloss_dA"]))
+    assert rel(xb, d["x0_bar"]) < 1e-11
+    assert rel(Fb, d["F0_bar"]) < 1e-11
 
 
 def _ext_scene():

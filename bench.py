@@ -143,7 +143,10 @@ def cpu_baseline(scenes, seconds):
         tot_t += t
     return {"value": tot_u / max(tot_t, 1e-9), "unit": UNIT, "cores": 1, "kind": "port",
             "sample": f"{len(picked)} smallest scenes of the workload ({tot_u} particle-steps), {steps} steps "
-                      f"fwd+adj each, numpy FP64 oracle, 1 thread"}
+                      f"fwd+adj each, numpy FP64 oracle, 1 thread",
+            "note": "the port vectorises the reference's per-particle numpy loops; the reference's own "
+                    "transfer.step + step_vjp ran at about 465 particle-steps/s on one core of the build "
+                    "machine (config-1 cube), so the port is far faster than the reference itself"}
 
 
 def cpp_reference_forward(seconds=4.0):
@@ -287,7 +290,9 @@ def main():
     scn = [scn_all[i] for i in mine]
     n_tot = sum(s["x"].shape[0] for s in scn)
     ck = a.ckpt_every if a.ckpt_every in ("auto", "sqrt") else int(a.ckpt_every)
-    tuning = load_tuned(scn, torch.float32) or {}
+    # the schedule tuned for this GPU (python -m morphompm_b200.batch --autotune);
+    # a rank's shard of a larger batch takes the 1-GPU batch's schedule
+    tuning = load_tuned(scn, torch.float32) or load_tuned(scn_all[:a.scenes], torch.float32) or {}
     slab_np = host_slab(scn, np.float32)
     b = Batch(scn, a.mpm_steps, dtype=torch.float32, ckpt_every=ck, tuning=tuning, slab_host=slab_np)
     k = b.ckpt_every

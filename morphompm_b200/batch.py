@@ -351,3 +351,24 @@ def autotune(scenes: List[dict], dtype=torch.float32, steps: int = 4, budget_s: 
         table.setdefault(_gpu_name(), {})[_signature(scenes, dtype)] = best
         json.dump(table, open(TUNE_CACHE, "w"), indent=1, sort_keys=True)
     return dict(best, _ms=t_best)
+
+
+def main():
+    """python -m morphompm_b200.batch --autotune [--scenes 256] [--budget 120]:
+    tune the config-4 batch on this GPU and store the schedule in tuned.json."""
+    import argparse
+    from . import scenes as S
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--autotune", action="store_true")
+    ap.add_argument("--scenes", type=int, default=256)
+    ap.add_argument("--budget", type=float, default=120.0)
+    ap.add_argument("--dtype", default="float32", choices=["float32", "float64"])
+    a = ap.parse_args()
+    if a.autotune:
+        dt = torch.float32 if a.dtype == "float32" else torch.float64
+        best = autotune(S.config4(n_scenes=a.scenes), dt, budget_s=a.budget, save=True, verbose=True)
+        print(json.dumps(best))
+
+
+if __name__ == "__main__":
+    main()

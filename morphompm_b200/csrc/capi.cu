@@ -226,19 +226,6 @@ int launch_nodes(MpmPlan* P, int mode, const Ctx& ctx, const int* active, const 
     return cudaLaunchKernel(f2, dim3(ctas), dim3(1024), a2, 0, st) == cudaSuccess ? MPM_OK : MPM_ERR_CUDA;
 }
 
-// P2G phase 1 from records staged in shared memory (schedule scatter_oxb = -1):
-// one warp per STAGE_CPW occupied cells, a persistent grid of CTAs
-template <typename R, int MODE>
-void launch_staged(MpmPlan* P, const Ctx& ctx, const unsigned* perm, const R* payload, const MpmParticles& in,
-                   const MpmCotangents& ob, int advect, cudaStream_t st) {
-    R* S = at<R>(P, P->o_sums);
-    const long long cap = P->n;
-    const long long chunks = (P->n + STAGE_CPW - 1) / STAGE_CPW;      // an upper bound of the cell chunks
-    const long long want = (chunks + STAGE_WARPS - 1) / STAGE_WARPS;
-    const int blocks = (int)std::max<long long>(1, std::min<long long>(want, (long long)P->n_sm * 16));
-    cell_sums_staged_kernel<R, MODE><<<blocks, 32 * STAGE_WARPS, 0, st>>>(ctx, perm, payload, in, ob, S, cap, advect);
-}
-
 // two-phase P2G: per-cell stencil sums, then per-node gather + grid epilogue
 template <typename R>
 int launch_p2g(MpmPlan* P, int mode, const Ctx& ctx, const unsigned* perm, const R* payload, const int* active,
@@ -248,13 +235,9 @@ int launch_p2g(MpmPlan* P, int mode, const Ctx& ctx, const unsigned* perm, const
     long long cap = P->n;
     int blocks1 = (int)std::min<long long>((P->n + 127) / 128, (long long)P->n_sm * 16);
     blocks1 = std::max(1, blocks1);
-    if (mode == 0 && P->tune.scatter_oxb == -1) {
-        launch_staged<R, 0>(P, ctx, perm, payload, MpmParticles{}, MpmCotangents{}, advect, st);
-    } else {
-        void* f1 = mode == 0 ? sums_fn<R, 0>(P->tune.scatter_oxb) : sums_fn<R, 1>(P->tune.scatter_oxb);
-        void* a1[] = {(void*)&ctx, (void*)&perm, (void*)&payload, (void*)&S, (void*)&cap};
-        if (cudaLaunchKernel(f1, dim3(blocks1), dim3(128), a1, 0, st) != cudaSuccess) return MPM_ERR_CUDA;
-    }
+    void* f1 = mode == 0 ? sums_fn<R, 0>(P->tune.scatter_oxb) : sums_fn<R, 1>(P->tune.scatter_oxb);
+    void* a1[] = {(void*)&ctx, (void*)&perm, (void*)&payload, (void*)&S, (void*)&cap};
+    if (cudaLaunchKernel(f1, dim3(blocks1), dim3(128), a1, 0, st) != cudaSuccess) return MPM_ERR_CUDA;
     P->launches += 1;   // the Site around this call counts one
     return launch_nodes<R>(P, mode, ctx, active, nact, grid_out, grid_fwd, advect, st);
 }
@@ -350,9 +333,7 @@ int step_bwd_R(MpmPlan* P, const MpmParticles& in, const void* outC, const MpmCo
         long long cap = P->n;
         int blocks1 = (int)std::min<long long>((P->n + 127) / 128, (long long)P->n_sm * 16);
         blocks1 = std::max(1, blocks1);
-        if (P->tune.scatter_oxb == -1)
-            launch_staged<R, 1>(P, ctx, tp.perm, nullptr, in, ob, advect, st);
-        else if (P->tune.scatter_oxb == 3 && sizeof(R) == 4)
+        if (P->tune.scatter_oxb == 3 && sizeof(R) == 4)
             cell_sums_adj_kernel<R, 3><<<blocks1, 128, 0, st>>>(ctx, tp.perm, in, ob, S, cap, advect);
         else
             cell_sums_adj_kernel<R, 1><<<blocks1, 128, 0, st>>>(ctx, tp.perm, in, ob, S, cap, advect);
@@ -441,9 +422,8 @@ int mpm_plan_create(const MpmScene* scenes, int32_t n_scenes, int32_t real_bytes
     if (P->tune.tile_xy != 8 && P->tune.tile_xy != 16) P->tune.tile_xy = 4;
     if (P->tune.tile_z != 8 && P->tune.tile_z != 16) P->tune.tile_z = 4;
     if (P->tune.scatter_ctas_per_sm <= 0) P->tune.scatter_ctas_per_sm = 1;
-    if (P->tune.scatter_oxb != -1 && P->tune.scatter_oxb != 1 && P->tune.scatter_oxb != 3)
-        P->tune.scatter_oxb = real_bytes == 4 ? 3 : 1;
-    if (real_bytes == 8 && P->tune.scatter_oxb == 3) P->tune.scatter_oxb = 1;
+    if (P->tune.scatter_oxb != 1 && P->tune.scatter_oxb != 3) P->tune.scatter_oxb = real_bytes == 4 ? 3 : 1;
+    if (real_bytes == 8) P->tune.scatter_oxb = 1;
     // the per-particle kernels are compiled for at most 256 threads per block
     if (P->tune.particle_block != 64 && P->tune.particle_block != 128) P->tune.particle_block = 256;
     if (P->tune.fp64_gap_thresh == 0.0f) P->tune.fp64_gap_thresh = 1e-6f;

@@ -30,17 +30,6 @@ namespace mpm {
 
 constexpr int PAYLOAD = 16;   // fx[3], m, a[3], B[9]
 
-// MPM_NODE_CLAMP: G2P and the reverse particle kernel walk the 27 stencil
-// nodes without per-node branches (DenseStencil::init_clamped)
-#ifndef MPM_NODE_CLAMP
-#define MPM_NODE_CLAMP 0
-#endif
-#if MPM_NODE_CLAMP
-#define MPM_NODE_SKIP(valid)
-#else
-#define MPM_NODE_SKIP(valid) if (!(valid)) continue
-#endif
-
 template <typename R> struct Vec4;
 template <> struct Vec4<float> { using T = float4; };
 template <> struct Vec4<double> { using T = double2; };
@@ -568,110 +557,6 @@ cell_sums_kernel(Ctx ctx, const unsigned* __restrict__ perm, const R* __restrict
 }
 
 // ---------------------------------------------------------------------------
-// P2G phase 1, staged (schedule scatter_oxb = -1).  Each warp takes STAGE_CPW
-// consecutive occupied cells.  Their particles are a contiguous run of sorted
-// slots: the warp brings their records into shared memory particle-parallel
-// (lane j takes slot j, so the loads are coalesced), then three lanes per cell,
-// one stencil x-offset each, add the records of the cell in sorted order.
-// MODE 0 copies the forward P2G records; MODE 1 forms the reverse record of
-// each particle there (see reverse_record).  The sums and their order are
-// those of the one-thread-per-cell kernels.
-// ---------------------------------------------------------------------------
-constexpr int STAGE_CPW = 10;     // cells per warp (30 of 32 lanes accumulate)
-constexpr int STAGE_WARPS = 4;    // warps per CTA
-template <typename R> struct StageCap { static constexpr int v = sizeof(R) == 4 ? 128 : 64; };
-
-// Reverse record of particle p (transfer.py:99-119): fx, -, nv_b, B with
-// nv_b = vn_b + dt xn_b (advect) and B = 4 inv_dx^2 dx (Cn_b + dt Fn_b F^T),
-// laid out like a forward record so accumulate_record<R, 1, .> reads it.
-template <typename R>
-__device__ __forceinline__ void reverse_record(const Ctx& ctx, const MpmParticles& in, const MpmCotangents& ob,
-                                               long long p, const MpmScene& sc, int advect, R r[PAYLOAD]) {
-    const R dx = (R)sc.dx, dt = (R)sc.dt, inv_dx = (R)(1.0 / sc.dx);
-    const R kdx = R(4) * inv_dx * inv_dx * dx;
-    R x[3], nv[3];
-    ld3<R>(in.x, p, in.sp3, in.sc3, x);
-    R F[9], Fb[9], Cb[9];
-    ld9<R>(in.F, p, in.sp9, in.sc9, F);
-    ld9<R>(ob.F, p, ob.sp9, ob.sc9, Fb);
-    ld9<R>(ob.C, p, ob.sp9, ob.sc9, Cb);
-    ld3<R>(ob.v, p, ob.sp3, ob.sc3, nv);
-    if (advect) {
-        R xb[3];
-        ld3<R>(ob.x, p, ob.sp3, ob.sc3, xb);
-#pragma unroll
-        for (int i = 0; i < 3; ++i) nv[i] += dt * xb[i];
-    }
-    R FbFt[9];
-    mmT(Fb, F, FbFt);
-    int base[3];
-    bin_particle(x, inv_dx, sc.shape, base, r);
-    r[3] = R(0);
-#pragma unroll
-    for (int i = 0; i < 3; ++i) r[4 + i] = nv[i];
-#pragma unroll
-    for (int i = 0; i < 9; ++i) r[7 + i] = kdx * (Cb[i] + dt * FbFt[i]);
-}
-
-template <typename R, int MODE>
-__global__ void __launch_bounds__(32 * STAGE_WARPS)
-cell_sums_staged_kernel(Ctx ctx, const unsigned* __restrict__ perm, const R* __restrict__ payload,
-                        MpmParticles in, MpmCotangents ob, R* __restrict__ S, long long cap, int advect) {
-    constexpr int CAP = StageCap<R>::v;
-    constexpr int LD = CAP + CAP / 8;      // one pad word per 8 slots: the cells' rows fall in distinct banks
-    __shared__ R rec_s[STAGE_WARPS][PAYLOAD][LD];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    R(*rs)[LD] = rec_s[warp];
-    const int nseg = *ctx.n_seg;
-    const int nchunk = (nseg + STAGE_CPW - 1) / STAGE_CPW;
-    const int cl = lane / 3, ox = lane - 3 * (lane / 3);
-    for (int chunk = blockIdx.x * STAGE_WARPS + warp; chunk < nchunk; chunk += gridDim.x * STAGE_WARPS) {
-        const int s0 = chunk * STAGE_CPW;
-        const int s1 = min(s0 + STAGE_CPW, nseg);
-        const int q0 = ctx.seg_first[s0], q1 = ctx.seg_last[s1 - 1];
-        if (!(MPM_INB(q0, ctx.n + 1, 11) && MPM_INB(q1, ctx.n + 1, 11))) continue;
-        const bool mine = lane < 3 * STAGE_CPW && s0 + cl < s1;
-        int f = 0, e = 0;
-        if (mine) {
-            f = ctx.seg_first[s0 + cl];
-            e = ctx.seg_last[s0 + cl];
-        }
-        R acc[1][3][3][4];
-        zero_acc<R, 1>(acc);
-        for (int r0 = q0; r0 < q1; r0 += CAP) {
-            const int len = min(CAP, q1 - r0);
-            __syncwarp();
-            for (int j = lane; j < len; j += 32) {
-                R r[PAYLOAD];
-                const long long p = perm[r0 + j];
-                if (!MPM_INB(p, ctx.n, 9)) continue;
-                if constexpr (MODE == 0) {
-                    load_record(payload, p, r);
-                } else {
-                    const MpmScene& sc = ctx.scenes[ctx.scene_of[r0 + j]];
-                    reverse_record<R>(ctx, in, ob, p, sc, advect, r);
-                }
-                const int jj = j + (j >> 3);
-#pragma unroll
-                for (int k = 0; k < PAYLOAD; ++k) rs[k][jj] = r[k];
-            }
-            __syncwarp();
-            if (mine) {
-                const int a = max(f, r0), b = min(e, r0 + len);
-                for (int q = a; q < b; ++q) {
-                    const int j = q - r0, jj = j + (j >> 3);
-                    R r[PAYLOAD];
-#pragma unroll
-                    for (int k = 0; k < PAYLOAD; ++k) r[k] = rs[k][jj];
-                    accumulate_record<R, MODE, 1>(r, ox, acc);
-                }
-            }
-        }
-        if (mine) store_acc<R, 1>(S, cap, s0 + cl, ox, acc);     // MODE 1 leaves channel 3 at zero
-    }
-}
-
-// ---------------------------------------------------------------------------
 // Reverse P2G, phase 1 (transfer.py:99-119 scatter of gv_b): per occupied cell
 // the 27 stencil sums of w (nv_b + k4 Cn_b' dp), with nv_b = vn_b + dt xn_b
 // (advect) and Cn_b' = Cn_b + dt Fn_b F^T formed here from the cotangents of
@@ -903,30 +788,6 @@ struct DenseStencil {
             oz[o] = k;
         }
     }
-    // Stencil of a particle whose base is inside the grid (bin_particle's
-    // `inside`): an offset that leaves the grid gets weight 0 and the index of
-    // the nearest in-grid node of the same stencil, which this step wrote, so
-    // the node loops need no per-node branch.
-    template <typename R>
-    __device__ __forceinline__ void init_clamped(const MpmScene& sc, const SceneAux& ax, const int base[3],
-                                                 R w[3][3], R dw[3][3]) {
-        const long long ny = sc.shape[1], nz = sc.shape[2];
-#pragma unroll
-        for (int o = 0; o < 3; ++o) {
-            const int i = base[0] + o, j = base[1] + o, k = base[2] + o;
-            vx[o] = i >= 0 && i < sc.shape[0];
-            vy[o] = j >= 0 && j < sc.shape[1];
-            vz[o] = k >= 0 && k < sc.shape[2];
-            const int ic = min(max(i, 0), sc.shape[0] - 1), jc = min(max(j, 0), sc.shape[1] - 1),
-                      kc = min(max(k, 0), sc.shape[2] - 1);
-            ox[o] = ax.node_begin + (long long)ic * ny * nz;
-            oy[o] = (long long)jc * nz;
-            oz[o] = kc;
-            if (!vx[o]) { w[o][0] = R(0); if (dw) dw[o][0] = R(0); }
-            if (!vy[o]) { w[o][1] = R(0); if (dw) dw[o][1] = R(0); }
-            if (!vz[o]) { w[o][2] = R(0); if (dw) dw[o][2] = R(0); }
-        }
-    }
 };
 
 __device__ __forceinline__ void unmark_cell(const Ctx& ctx, const SceneAux& ax, const unsigned* __restrict__ skeys,
@@ -957,31 +818,26 @@ g2p_kernel(Ctx ctx, Tape<R> tp, MpmParticles in, MpmParticles out, int advect, u
     ld3<R>(in.x, p, in.sp3, in.sc3, x);
     int base[3];
     R fx[3];
-    const bool inside = bin_particle(x, inv_dx, sc.shape, base, fx);
+    bin_particle(x, inv_dx, sc.shape, base, fx);
     R w[3][3];
     bspline(fx, w);
     DenseStencil st;
-#if MPM_NODE_CLAMP
-    st.init_clamped<R>(sc, ax, base, w, nullptr);
-#else
     st.init(sc, ax, base);
-#endif
     const R* __restrict__ dense = static_cast<const R*>(ctx.dense_f);
     // nC = k4 sum w g (o - fx)^T dx = k4 dx (G - nv fx^T),  G[i][d] = sum w g_i o_d
     R nv[3] = {0, 0, 0}, G[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-    if (!MPM_NODE_CLAMP || inside)
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-        MPM_NODE_SKIP(st.vx[a]);
+        if (!st.vx[a]) continue;
 #pragma unroll
         for (int b = 0; b < 3; ++b) {
-            MPM_NODE_SKIP(st.vy[b]);
+            if (!st.vy[b]) continue;
             const long long rab = st.ox[a] + st.oy[b];
             // column sums over z: sum w_c g and sum c w_c g
             R Zg[3] = {0, 0, 0}, Zc[3] = {0, 0, 0};
 #pragma unroll
             for (int c = 0; c < 3; ++c) {
-                MPM_NODE_SKIP(st.vz[c]);
+                if (!st.vz[c]) continue;
                 R g[4];
                 if (!MPM_INB(rab + st.oz[c], ctx.n_nodes, 7)) continue;
                 load_node(dense, rab + st.oz[c], g);
@@ -1110,16 +966,12 @@ bwd_particle_kernel(Ctx ctx, Tape<R> tp, MpmParticles in, const R* __restrict__ 
     }
     int base[3];
     R fx[3];
-    const bool inside = bin_particle(x, inv_dx, sc.shape, base, fx);
+    bin_particle(x, inv_dx, sc.shape, base, fx);
     R w[3][3], dw[3][3];
     bspline(fx, w);
     bspline_grad(fx, dw);
     DenseStencil st;
-#if MPM_NODE_CLAMP
-    st.init_clamped<R>(sc, ax, base, w, dw);
-#else
     st.init(sc, ax, base);
-#endif
 
     // The node loop is evaluated as separable sums: per stencil column (a,b)
     // the z-weighted sums of gv, mb and c*mb, and of the advect factor
@@ -1140,13 +992,12 @@ bwd_particle_kernel(Ctx ctx, Tape<R> tp, MpmParticles in, const R* __restrict__ 
     R xs[3] = {0, 0, 0}, wgv[3] = {0, 0, 0}, wmb[3] = {0, 0, 0}, GB[9];
 #pragma unroll
     for (int q = 0; q < 9; ++q) GB[q] = R(0);
-    if (!MPM_NODE_CLAMP || inside)
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-        MPM_NODE_SKIP(st.vx[a]);
+        if (!st.vx[a]) continue;
 #pragma unroll
         for (int b = 0; b < 3; ++b) {
-            MPM_NODE_SKIP(st.vy[b]);
+            if (!st.vy[b]) continue;
             const long long rab = st.ox[a] + st.oy[b];
             R Zg[3] = {0, 0, 0}, Zm[3] = {0, 0, 0}, Zc[3] = {0, 0, 0}, Sab = 0, Tab = 0;
             R Uab[3], Vab[3];
@@ -1157,7 +1008,7 @@ bwd_particle_kernel(Ctx ctx, Tape<R> tp, MpmParticles in, const R* __restrict__ 
             }
 #pragma unroll
             for (int cc = 0; cc < 3; ++cc) {
-                MPM_NODE_SKIP(st.vz[cc]);
+                if (!st.vz[cc]) continue;
                 R gf[4], gb[4];
                 if (!MPM_INB(rab + st.oz[cc], ctx.n_nodes, 7)) continue;
                 load_node(dfw, rab + st.oz[cc], gf);

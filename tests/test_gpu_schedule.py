@@ -1,6 +1,6 @@
 """Schedules do not change results: every schedule knob of the autotuner (node
-tile shape, particle block size, stencil x-offsets per pass of the P2G phase-1
-kernels, records staged in shared memory) gives bitwise the default
+tile shape, particle block size, P2G node-gather CTAs per SM, stencil
+x-offsets per pass of the P2G phase-1 kernels) gives bitwise the default
 schedule's losses, growth gradients and final state on a small uneven batch.
 The per-node sum order (source cells o = 0..26) and the per-cell order
 (sorted particles) are fixed whatever the schedule."""
@@ -14,7 +14,6 @@ SCHEDULES = [
     {"tile_xy": 8, "tile_z": 16, "particle_block": 128},
     {"tile_xy": 4, "tile_z": 8, "scatter_ctas_per_sm": 2},
     {"scatter_oxb": 1},
-    {"scatter_oxb": -1},
 ]
 
 

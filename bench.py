@@ -44,6 +44,7 @@ def parse():
                     help="checkpoint interval: an int, 'sqrt', or 'auto' (largest that fits 75%% of free HBM)")
     ap.add_argument("--no-plain", action="store_true", help="skip the FP64 plain-path leg")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-others", action="store_true", help="skip the configs 1, 2, 3, 5 leg")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--workload", default="config4", choices=["config1", "config2", "config3", "config4", "config5"],
                     help="config4 is the headline line; the others print one line each for the other growth "
@@ -420,11 +421,27 @@ def main():
             "device_status": status, "active_tile_cap": plan.tuning.get("active_tile_cap"),
             "gathered": gathered}
 
-    if rank == 0 and not a.no_plain:
+    # the 1-GPU legs (FP64 plain path, CPU baselines, the other workloads)
+    if world == 1 and not a.no_plain:
         line["fp64_plain"] = plain_leg(scn, a, value, peak, tuning)
-    if rank == 0 and not a.no_cpu:
+    if world == 1 and not a.no_cpu:
         line["cpu_baseline"] = cpu_baseline(scn, a.cpu_seconds)
         line["cpu_reference_forward"] = cpp_reference_forward()
+    if world == 1 and not a.no_others:
+        # the other growth workloads, one timed trajectory each after one warm-up
+        b.graph = None
+        del b
+        torch.cuda.empty_cache()
+        others = {}
+        for w in ("config1", "config2", "config3", "config5"):
+            r = workload_line(w, 1, 1)
+            others[w] = {"name": r["name"], "particles": r["particles"], "mpm_steps": r["mpm_steps"],
+                         "results": {k: {kk: v[kk] for kk in ("value", "ms_per_trajectory", "ckpt_every",
+                                                              "trajectory_storage_gb", "device_status")}
+                                     for k, v in r["results"].items()},
+                         "fp32_error_vs_fp64": r.get("fp32_error_vs_fp64")}
+            torch.cuda.empty_cache()
+        line["other_workloads"] = others
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:
@@ -468,15 +485,20 @@ def _curvature(final_slab):
 
 def run_other(a):
     """One JSON line for configs 1, 2, 3 or 5 (particle-steps/s fwd+adj)."""
+    print(json.dumps(workload_line(a.workload, a.steps, a.warmup)), flush=True)
+
+
+def workload_line(w, steps, warmup):
+    """Throughput of one of configs 1, 2, 3, 5 (FP64 and FP32 where the
+    workload names both), with the FP32 error against FP64."""
     import torch
     from morphompm_b200 import scenes as S
     from morphompm_b200.batch import Batch, host_slab
     from morphompm_b200.trajectory import sqrt_schedule
-    w = a.workload
     c = getattr(S, w)()
     n = c["x"].shape[0]
-    line = {"metric": METRIC, "unit": UNIT, "workload": w, "name": c["name"], "n_gpus": 1, "steps": a.steps,
-            "warmup": a.warmup, "higher_is_better": True, "data": "synthetic", "particles": n,
+    line = {"metric": METRIC, "unit": UNIT, "workload": w, "name": c["name"], "n_gpus": 1, "steps": steps,
+            "warmup": warmup, "higher_is_better": True, "data": "synthetic", "particles": n,
             "mpm_steps": c["steps"], "results": {}}
     loss, x_obs = "detF", None
     if w == "config3":
@@ -502,7 +524,7 @@ def run_other(a):
             b = Batch([c], c["steps"], dtype=dt, ckpt_every=ck, loss=loss, x_obs=x_obs)
         npd = np.float64 if dt == torch.float64 else np.float32
         b.load(host_slab([c], npd), non_blocking=False)
-        ms = _timed_trajectories(b, a.steps, a.warmup)
+        ms = _timed_trajectories(b, steps, warmup)
         key = "fp64" if dt == torch.float64 else "fp32"
         mem = b.rollout.memory_bytes() + b.plan.ws_bytes
         res = {"value": n * c["steps"] / (ms / 1e3), "ms_per_trajectory": ms, "ckpt_every": b.ckpt_every,
@@ -525,7 +547,7 @@ def run_other(a):
     main_key = "fp32" if "fp32" in line["results"] else "fp64"
     line["value"] = line["results"][main_key]["value"]
     line["dtype"] = "f32" if main_key == "fp32" else "f64"
-    print(json.dumps(line), flush=True)
+    return line
 
 
 def plain_leg(scn, a, value32, peak, tuning32=None):

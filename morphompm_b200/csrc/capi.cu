@@ -52,6 +52,11 @@ struct MpmPlan {
     size_t o_scenes, o_aux, o_scene_of, o_tile_scene, o_status, o_cell_seg, o_blk, o_tblk;
     size_t o_tile_flag, o_keys, o_kalt0, o_valt0, o_kalt1, o_valt1, o_hist, o_totals, o_payload, o_sums;
     size_t o_dense_f = 0, o_dense_b = 0;
+    // incremental re-sort of chained steps (SIZE_MAX: not laid out)
+    size_t o_mflag = SIZE_MAX, o_pflag = 0, o_mask = 0, o_pmask = 0, o_wpre = 0, o_rblk = 0, o_pblk = 0;
+    size_t o_mkey = 0, o_mpart = 0, o_okey = 0, o_opart = 0, o_rint = 0;
+    int nblk_resort = 1;
+    char* chain_tape = nullptr;    // the tape whose sorted order the emitted mover flags refer to
     long long n_nodes = 0;
     size_t o_dbuf, o_tape;
     int nblk_seg = 1, nblk_tile = 1;
@@ -105,6 +110,8 @@ Ctx make_ctx(MpmPlan* P) {
     c.ext_tau_bar = P->ext_tau_bar;
     c.dense_f = P->ws + P->o_dense_f;
     c.dense_b = P->ws + P->o_dense_b;
+    c.mover_flag = P->o_mflag == SIZE_MAX ? nullptr : at<unsigned char>(P, P->o_mflag);
+    c.mover_pflag = P->o_mflag == SIZE_MAX ? nullptr : at<unsigned char>(P, P->o_pflag);
     c.n = P->n;
     c.n_tiles = P->n_tiles;
     c.n_keys = P->n_keys;
@@ -242,27 +249,87 @@ int launch_p2g(MpmPlan* P, int mode, const Ctx& ctx, const unsigned* perm, const
     return launch_nodes<R>(P, mode, ctx, active, nact, grid_out, grid_fwd, advect, st);
 }
 
-// stable LSD radix sort of the binning keys -> tape (skeys, perm)
-int run_sort(MpmPlan* P, const unsigned* keys, unsigned* skeys, unsigned* perm, cudaStream_t st) {
-    unsigned* kalt[2] = {at<unsigned>(P, P->o_kalt0), at<unsigned>(P, P->o_kalt1)};
-    unsigned* valt[2] = {at<unsigned>(P, P->o_valt0), at<unsigned>(P, P->o_valt1)};
+// Stable LSD radix sort of kin (with payload vin, or the index when null)
+// into (kout, vout), through the alternate buffers a0 and a1 (a1 may be the
+// input's own buffers).  n_dev: sort the first *n_dev keys (a device count).
+int run_radix(MpmPlan* P, const unsigned* kin, const unsigned* vin, unsigned* kout, unsigned* vout, unsigned* a0k,
+              unsigned* a0v, unsigned* a1k, unsigned* a1v, const int* n_dev, cudaStream_t st) {
     unsigned* hist = at<unsigned>(P, P->o_hist);
     unsigned* totals = at<unsigned>(P, P->o_totals);
     const int nblk = P->nblk_sort;
-    const unsigned* ksrc = keys;
-    const unsigned* vsrc = nullptr;
-    Site site(P, MPM_K_SORT, 4 * P->passes, st);
+    const unsigned* ksrc = kin;
+    const unsigned* vsrc = vin;
     for (int pass = 0; pass < P->passes; ++pass) {
         const int shift = pass * RADIX_BITS;
-        unsigned* kdst = (pass == P->passes - 1) ? skeys : kalt[pass & 1];
-        unsigned* vdst = (pass == P->passes - 1) ? perm : valt[pass & 1];
-        radix_hist_kernel<<<nblk, SORT_THREADS, 0, st>>>(ksrc, P->n, shift, hist, nblk);
-        radix_rowsum_kernel<<<RADIX, 256, 0, st>>>(hist, nblk, totals);
-        radix_rowscan_kernel<<<RADIX, 256, 0, st>>>(hist, nblk, totals);
-        radix_scatter_kernel<<<nblk, SORT_THREADS, 0, st>>>(ksrc, vsrc, P->n, shift, hist, nblk, kdst, vdst);
+        const bool last = pass == P->passes - 1;
+        unsigned* kdst = last ? kout : ((pass & 1) ? a1k : a0k);
+        unsigned* vdst = last ? vout : ((pass & 1) ? a1v : a0v);
+        radix_hist_kernel<<<nblk, SORT_THREADS, 0, st>>>(ksrc, P->n, shift, hist, nblk, n_dev);
+        radix_rowsum_kernel<<<RADIX, 256, 0, st>>>(hist, nblk, totals, n_dev);
+        radix_rowscan_kernel<<<RADIX, 256, 0, st>>>(hist, nblk, totals, n_dev);
+        radix_scatter_kernel<<<nblk, SORT_THREADS, 0, st>>>(ksrc, vsrc, P->n, shift, hist, nblk, kdst, vdst, n_dev);
         ksrc = kdst;
         vsrc = vdst;
     }
+    return check_launch();
+}
+
+// stable LSD radix sort of the binning keys -> tape (skeys, perm)
+int run_sort(MpmPlan* P, const unsigned* keys, unsigned* skeys, unsigned* perm, cudaStream_t st) {
+    Site site(P, MPM_K_SORT, 4 * P->passes, st);
+    return run_radix(P, keys, nullptr, skeys, perm, at<unsigned>(P, P->o_kalt0), at<unsigned>(P, P->o_valt0),
+                     at<unsigned>(P, P->o_kalt1), at<unsigned>(P, P->o_valt1), nullptr, st);
+}
+
+// Sorted order of a chained step from the previous step's (old_tape) and the
+// mover flags its emitting G2P wrote (sort.cuh, incremental re-sort): the
+// movers, gathered in particle order, are radix-sorted by key on their
+// device-side count and merged with the slots that kept their key.
+int run_resort(MpmPlan* P, const char* old_tape, char* tape, const unsigned* keys, cudaStream_t st) {
+    const unsigned* ok = reinterpret_cast<const unsigned*>(old_tape + P->t_skeys);
+    const unsigned* op = reinterpret_cast<const unsigned*>(old_tape + P->t_perm);
+    unsigned* nk = reinterpret_cast<unsigned*>(tape + P->t_skeys);
+    unsigned* np = reinterpret_cast<unsigned*>(tape + P->t_perm);
+    const size_t nb4 = (size_t)P->n * 4;
+    if (old_tape == tape) {
+        // the old order is overwritten by the new one: read it from a copy
+        unsigned* ck = at<unsigned>(P, P->o_kalt0);
+        unsigned* cp = at<unsigned>(P, P->o_valt0);
+        if (cudaMemcpyAsync(ck, ok, nb4, cudaMemcpyDeviceToDevice, st) != cudaSuccess ||
+            cudaMemcpyAsync(cp, op, nb4, cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+            return MPM_ERR_CUDA;
+        ok = ck;
+        op = cp;
+    }
+    unsigned* mask = at<unsigned>(P, P->o_mask);
+    unsigned* pmask = at<unsigned>(P, P->o_pmask);
+    unsigned* wpre = at<unsigned>(P, P->o_wpre);
+    unsigned* rblk = at<unsigned>(P, P->o_rblk);
+    unsigned* pblk = at<unsigned>(P, P->o_pblk);
+    unsigned* mk = at<unsigned>(P, P->o_mkey);
+    unsigned* mp = at<unsigned>(P, P->o_mpart);
+    unsigned* sk = at<unsigned>(P, P->o_okey);
+    unsigned* sp = at<unsigned>(P, P->o_opart);
+    int* n_movers = at<int>(P, P->o_rint);
+    const unsigned char* sflag = at<const unsigned char>(P, P->o_mflag);
+    const unsigned char* pflag = at<const unsigned char>(P, P->o_pflag);
+    int* status = at<int>(P, P->o_status);
+    Site site(P, MPM_K_SORT, 7 + 4 * P->passes, st);
+    const int nb = P->nblk_resort;
+    resort_count_kernel<<<nb, RESORT_THREADS, 0, st>>>(sflag, pflag, P->n, mask, pmask, rblk, pblk);
+    scan_counts_kernel<<<1, 1024, 0, st>>>(rblk, nb, n_movers + 1, INT_MAX, status);
+    scan_counts_kernel<<<1, 1024, 0, st>>>(pblk, nb, n_movers, INT_MAX, status);
+    resort_compact_kernel<<<nb, RESORT_THREADS, 0, st>>>(mask, pmask, P->n, rblk, pblk, keys, wpre, mk, mp);
+    int rc = check_launch();
+    if (rc) return rc;
+    // movers in particle order -> (key, particle) order; the second alternate is the input's buffers
+    rc = run_radix(P, mk, mp, sk, sp, at<unsigned>(P, P->o_kalt1), at<unsigned>(P, P->o_valt1), mk, mp, n_movers,
+                   st);
+    if (rc) return rc;
+    resort_place_stayers_kernel<<<grid_for(P->n, RESORT_THREADS), RESORT_THREADS, 0, st>>>(
+        mask, wpre, P->n, ok, op, sk, sp, n_movers, nk, np);
+    const int gm = (int)std::max<long long>(1, std::min<long long>(grid_for(P->n, RESORT_THREADS), (long long)P->n_sm * 8));
+    resort_place_movers_kernel<<<gm, RESORT_THREADS, 0, st>>>(mask, wpre, P->n, ok, op, sk, sp, n_movers, nk, np);
     return check_launch();
 }
 
@@ -280,7 +347,8 @@ int step_fwd_R(MpmPlan* P, const MpmParticles& in, MpmParticles& out, int advect
     unsigned* keys = at<unsigned>(P, P->o_keys);
     R* payload = at<R>(P, P->o_payload);
     if (!chained) { Site s(P, MPM_K_BIN, 1, st); bin_kernel<R><<<g, B, 0, st>>>(ctx, in, keys); }
-    int rc = run_sort(P, keys, tp.skeys, tp.perm, st);
+    int rc = chained && P->chain_tape && ctx.mover_flag ? run_resort(P, P->chain_tape, tape, keys, st)
+                                                        : run_sort(P, keys, tp.skeys, tp.perm, st);
     if (rc) return rc;
     rc = build_segments(P, ctx, tp.skeys, st);
     if (rc) return rc;
@@ -505,6 +573,20 @@ int mpm_plan_create(const MpmScene* scenes, int32_t n_scenes, int32_t real_bytes
     P->o_dense_f = L.take((size_t)P->n_nodes * 4 * R);
     P->o_dense_b = L.take((size_t)P->n_nodes * 4 * R);
     P->o_dbuf = L.take(3 * n * 8);      // dL/dA, dL/dmu, dL/dlambda per slot
+    const size_t nw = (n + 31) / 32;
+    P->nblk_resort = (int)((nw + RESORT_THREADS - 1) / RESORT_THREADS);
+    P->o_mflag = L.take(nw * 32);
+    P->o_pflag = L.take(nw * 32);
+    P->o_mask = L.take(nw * 4);
+    P->o_pmask = L.take(nw * 4);
+    P->o_wpre = L.take(nw * 4);
+    P->o_rblk = L.take((size_t)P->nblk_resort * 4);
+    P->o_pblk = L.take((size_t)P->nblk_resort * 4);
+    P->o_mkey = L.take(n * 4);
+    P->o_mpart = L.take(n * 4);
+    P->o_okey = L.take(n * 4);
+    P->o_opart = L.take(n * 4);
+    P->o_rint = L.take(8);
     P->o_tape = L.take(P->tape_bytes);
     P->ws_bytes = L.off;
     *out = P;
@@ -694,6 +776,7 @@ int mpm_step_fwd_chain(MpmPlan* P, const MpmParticles* in, MpmParticles* out, in
         P->chain_valid = true;
         P->chain_t = step_index + 1;
         P->chain_state = *out;
+        P->chain_tape = tp;
     }
     return rc;
 }

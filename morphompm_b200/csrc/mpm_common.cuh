@@ -71,6 +71,8 @@ struct Ctx {
     void* ext_tau_bar;           // and its cotangent, written by the reverse step (n x 9)
     void* dense_f;               // dense node scratch, forward record (m, v[3]) per node
     void* dense_b;               // dense node scratch, reverse record (gm_b, gmom_b[3]) per node
+    unsigned char* mover_flag;   // emitting G2P: per sorted slot, its particle changed cell (may be null)
+    unsigned char* mover_pflag;  // and the same flag per particle
     long long n;
     long long n_tiles;
     long long n_keys;            // padded cells of all scenes (cell_seg entries)

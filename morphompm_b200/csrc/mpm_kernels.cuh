@@ -888,7 +888,14 @@ g2p_kernel(Ctx ctx, Tape<R> tp, MpmParticles in, MpmParticles out, int advect, u
         // the next step's binning and P2G record of the new state (what the
         // bin and prepass kernels of step t+1 would compute from memory)
         R fxn[3], Fg[9], rec[PAYLOAD];
-        keys[p] = particle_key<R>(ctx, sc, ax, xn, fxn);
+        const unsigned kn = particle_key<R>(ctx, sc, ax, xn, fxn);
+        keys[p] = kn;
+        // movers of this step's sorted order (the next step's incremental re-sort)
+        if (ctx.mover_flag) {
+            const unsigned char moved = kn != tp.skeys[sidx] ? 1 : 0;
+            ctx.mover_flag[sidx] = moved;
+            ctx.mover_pflag[p] = moved;
+        }
         load_Fg<R>(ctx, sc, in, p, t + 1, Fg, nullptr);
         p2g_record<R>(ctx, sc, p, fxn, nv, nC, Fn, Fg, rec);
         store_record(payload, p, rec);

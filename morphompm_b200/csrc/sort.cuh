@@ -1,5 +1,8 @@
 // Deterministic, stable LSD radix sort of 32-bit cell keys with 32-bit payload
-// indices, and the tile-list compaction.  No global atomics: each pass builds
+// indices, and the incremental re-sort of a chained step.  Given n_dev, the
+// radix kernels sort the first *n_dev keys (a count formed on the device; the
+// launch is sized for n): blocks past it return and the digit scans cover the
+// blocks in use only.  No global atomics: each pass builds
 // per-block digit counts (shared-memory counters), scans them digit-major into
 // global offsets (row totals, then per-digit row scans) and scatters every key
 // to offset + its stable rank inside the block, ranked with warp match masks.
@@ -15,9 +18,20 @@ constexpr int SORT_THREADS = 256;
 constexpr int SORT_ITEMS = 16;                       // keys per thread per block
 constexpr int SORT_TILE = SORT_THREADS * SORT_ITEMS; // keys per block
 
+// Blocks of a sort over *n_dev keys (a count on the device; the grid and the
+// histogram stride are sized for nblk blocks), or nblk.
+__device__ __forceinline__ int active_blocks(int nblk, const int* __restrict__ n_dev) {
+    if (!n_dev) return nblk;
+    const long long a = ((long long)*n_dev + SORT_TILE - 1) / SORT_TILE;
+    return (int)(a < nblk ? a : nblk);
+}
+
 // Per-block digit histogram.  hist is digit-major: hist[d * nblk + b].
 __global__ void __launch_bounds__(SORT_THREADS)
-radix_hist_kernel(const unsigned* __restrict__ keys, long long n, int shift, unsigned* __restrict__ hist, int nblk) {
+radix_hist_kernel(const unsigned* __restrict__ keys, long long n, int shift, unsigned* __restrict__ hist, int nblk,
+                  const int* __restrict__ n_dev) {
+    if (n_dev) n = *n_dev;
+    if ((long long)blockIdx.x * SORT_TILE >= n && blockIdx.x > 0) return;
     __shared__ unsigned cnt[RADIX];
     for (int d = threadIdx.x; d < RADIX; d += SORT_THREADS) cnt[d] = 0;
     __syncthreads();
@@ -33,11 +47,13 @@ radix_hist_kernel(const unsigned* __restrict__ keys, long long n, int shift, uns
 
 // totals[d] = sum_b hist[d][b]   (one block per digit, fixed-order tree)
 __global__ void __launch_bounds__(256)
-radix_rowsum_kernel(const unsigned* __restrict__ hist, int nblk, unsigned* __restrict__ totals) {
+radix_rowsum_kernel(const unsigned* __restrict__ hist, int nblk, unsigned* __restrict__ totals,
+                    const int* __restrict__ n_dev) {
+    const int nact = active_blocks(nblk, n_dev);
     __shared__ unsigned red[256];
     int d = blockIdx.x;
     unsigned s = 0;
-    for (int b = threadIdx.x; b < nblk; b += 256) s += hist[(long long)d * nblk + b];
+    for (int b = threadIdx.x; b < nact; b += 256) s += hist[(long long)d * nblk + b];
     red[threadIdx.x] = s;
     __syncthreads();
     for (int w = 128; w > 0; w >>= 1) {
@@ -49,7 +65,9 @@ radix_rowsum_kernel(const unsigned* __restrict__ hist, int nblk, unsigned* __res
 
 // hist[d][b] <- sum_{d'<d} totals[d'] + sum_{b'<b} hist[d][b']   (one block per digit)
 __global__ void __launch_bounds__(256)
-radix_rowscan_kernel(unsigned* __restrict__ hist, int nblk, const unsigned* __restrict__ totals) {
+radix_rowscan_kernel(unsigned* __restrict__ hist, int nblk, const unsigned* __restrict__ totals,
+                     const int* __restrict__ n_dev) {
+    const int nact = active_blocks(nblk, n_dev);
     __shared__ unsigned sh[256];
     __shared__ unsigned carry;
     int d = blockIdx.x;
@@ -64,9 +82,9 @@ radix_rowscan_kernel(unsigned* __restrict__ hist, int nblk, const unsigned* __re
     }
     if (threadIdx.x == 0) carry = sh[0];
     __syncthreads();
-    for (int b0 = 0; b0 < nblk; b0 += 256) {
+    for (int b0 = 0; b0 < nact; b0 += 256) {
         int b = b0 + threadIdx.x;
-        unsigned v = (b < nblk) ? hist[(long long)d * nblk + b] : 0u;
+        unsigned v = (b < nact) ? hist[(long long)d * nblk + b] : 0u;
         sh[threadIdx.x] = v;
         __syncthreads();
         // Hillis-Steele inclusive scan
@@ -78,7 +96,7 @@ radix_rowscan_kernel(unsigned* __restrict__ hist, int nblk, const unsigned* __re
         }
         unsigned incl = sh[threadIdx.x];
         unsigned c = carry;
-        if (b < nblk) hist[(long long)d * nblk + b] = c + incl - v;
+        if (b < nact) hist[(long long)d * nblk + b] = c + incl - v;
         __syncthreads();
         if (threadIdx.x == 255) carry = c + incl;
         __syncthreads();
@@ -95,7 +113,9 @@ radix_rowscan_kernel(unsigned* __restrict__ hist, int nblk, const unsigned* __re
 __global__ void __launch_bounds__(SORT_THREADS)
 radix_scatter_kernel(const unsigned* __restrict__ keys_in, const unsigned* __restrict__ vals_in, long long n,
                      int shift, const unsigned* __restrict__ offs, int nblk,
-                     unsigned* __restrict__ keys_out, unsigned* __restrict__ vals_out) {
+                     unsigned* __restrict__ keys_out, unsigned* __restrict__ vals_out, const int* __restrict__ n_dev) {
+    if (n_dev) n = *n_dev;
+    if ((long long)blockIdx.x * SORT_TILE >= n) return;
     constexpr int NW = SORT_THREADS / 32;
     constexpr int PER_WARP = SORT_TILE / NW;   // SORT_ITEMS rounds of 32 keys
     __shared__ unsigned wcnt[NW][RADIX];
@@ -155,6 +175,195 @@ radix_scatter_kernel(const unsigned* __restrict__ keys_in, const unsigned* __res
         __syncwarp();
         if (valid && rank == 0) wcnt[warp][dig] = base + __popc(peers);
         __syncwarp();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Incremental re-sort of a chained step.  The sorted order is by (cell key,
+// particle index), the order of the stable radix sort of keys in particle
+// order.  Between two steps few particles change cell: the emitting G2P of
+// the previous step flags, per slot of the previous order and per particle,
+// whether the particle's new key differs from its old one (a "mover").  The
+// slots that keep their key ("stayers") are still in (key, particle) order.
+// The movers are gathered in particle order and stable-sorted by key with the
+// radix sort on their device-side count, which puts them in (key, particle)
+// order; then the two sorted sequences are merged: the stayer at old slot q
+// goes to q - (movers before q) + (movers ordered before it), mover i to
+// i + (stayers ordered before it).  The result is exactly the full sort's.
+// ---------------------------------------------------------------------------
+constexpr int RESORT_THREADS = 256;        // threads per block; one 32-slot mask word per thread
+
+// 32 flag bytes from index 32 w -> one mask word (bits of indices >= n clear)
+__device__ __forceinline__ unsigned pack_flags(const unsigned char* __restrict__ flag, long long w, long long n) {
+    const uint4* f = reinterpret_cast<const uint4*>(flag + (w << 5));
+    const uint4 a = f[0], b = f[1];
+    const unsigned wd[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+    unsigned m = 0;
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+            if ((wd[i] >> (8 * j)) & 0xffu) m |= 1u << (4 * i + j);
+    const long long rem = n - (w << 5);
+    if (rem < 32) m &= (1u << rem) - 1u;
+    return m;
+}
+
+__device__ __forceinline__ unsigned block_sum(unsigned c, unsigned* red) {
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = c;
+    __syncthreads();
+    unsigned t = 0;
+    for (int i = 0; i < RESORT_THREADS / 32; ++i) t += red[i];
+    return t;
+}
+
+// Mover flags -> mask words, per slot (old order) and per particle, and each
+// block's count of both.
+__global__ void __launch_bounds__(RESORT_THREADS)
+resort_count_kernel(const unsigned char* __restrict__ slot_flag, const unsigned char* __restrict__ part_flag,
+                    long long n, unsigned* __restrict__ slot_mask, unsigned* __restrict__ part_mask,
+                    unsigned* __restrict__ slot_blk, unsigned* __restrict__ part_blk) {
+    __shared__ unsigned red[2][RESORT_THREADS / 32];
+    const long long nw = (n + 31) >> 5;
+    const long long w = (long long)blockIdx.x * RESORT_THREADS + threadIdx.x;
+    unsigned ms = 0, mp = 0;
+    if (w < nw) {
+        ms = pack_flags(slot_flag, w, n);
+        mp = pack_flags(part_flag, w, n);
+        slot_mask[w] = ms;
+        part_mask[w] = mp;
+    }
+    const unsigned cs = block_sum(__popc(ms), red[0]);
+    const unsigned cp = block_sum(__popc(mp), red[1]);
+    if (threadIdx.x == 0) {
+        slot_blk[blockIdx.x] = cs;
+        part_blk[blockIdx.x] = cp;
+    }
+}
+
+// exclusive prefix of c over the block, from base
+__device__ __forceinline__ unsigned block_prefix(unsigned c, unsigned* sh) {
+    sh[threadIdx.x] = c;
+    __syncthreads();
+    for (int o = 1; o < RESORT_THREADS; o <<= 1) {
+        const unsigned t = threadIdx.x >= (unsigned)o ? sh[threadIdx.x - o] : 0u;
+        __syncthreads();
+        sh[threadIdx.x] += t;
+        __syncthreads();
+    }
+    const unsigned r = sh[threadIdx.x] - c;
+    __syncthreads();
+    return r;
+}
+
+// After the block offsets are scanned: the movers before each slot mask word
+// (wpre), and the movers' new keys and particle indices in particle order.
+__global__ void __launch_bounds__(RESORT_THREADS)
+resort_compact_kernel(const unsigned* __restrict__ slot_mask, const unsigned* __restrict__ part_mask, long long n,
+                      const unsigned* __restrict__ slot_blk, const unsigned* __restrict__ part_blk,
+                      const unsigned* __restrict__ keys, unsigned* __restrict__ wpre,
+                      unsigned* __restrict__ mkey, unsigned* __restrict__ mpart) {
+    __shared__ unsigned sh[RESORT_THREADS];
+    const long long nw = (n + 31) >> 5;
+    const long long w = (long long)blockIdx.x * RESORT_THREADS + threadIdx.x;
+    const unsigned ms = w < nw ? slot_mask[w] : 0u, mp = w < nw ? part_mask[w] : 0u;
+    const unsigned ps = block_prefix(__popc(ms), sh);
+    const unsigned pp = block_prefix(__popc(mp), sh);
+    if (w >= nw) return;
+    wpre[w] = slot_blk[blockIdx.x] + ps;
+    unsigned rest = mp, idx = part_blk[blockIdx.x] + pp;
+    while (rest) {
+        const int b = __ffs(rest) - 1;
+        rest &= rest - 1u;
+        const long long p = (w << 5) + b;
+        if (MPM_INB(idx, n, 10)) {
+            mkey[idx] = keys[p];
+            mpart[idx] = (unsigned)p;
+        }
+        ++idx;
+    }
+}
+
+// movers before slot q of the old order
+__device__ __forceinline__ unsigned resort_movers_before(const unsigned* __restrict__ mask,
+                                                         const unsigned* __restrict__ wpre, long long q,
+                                                         long long n, unsigned total) {
+    if (q >= n) return total;
+    const long long w = q >> 5;
+    const int b = (int)(q & 31);
+    return wpre[w] + __popc(mask[w] & ((1u << b) - 1u));
+}
+
+__device__ __forceinline__ unsigned long long pair_key(unsigned k, unsigned p) {
+    return ((unsigned long long)k << 32) | p;
+}
+
+// first sorted mover not ordered before v, in [lo, hi)
+__device__ __forceinline__ int mover_bound(const unsigned* __restrict__ mk, const unsigned* __restrict__ mp,
+                                           unsigned long long v, int lo, int hi) {
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (pair_key(mk[mid], mp[mid]) < v) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+
+// Stayers to their new slots.  The block's slots span a key range: its first
+// and last old (key, particle) values bound the movers ordered before any of
+// its stayers, so every thread searches that narrow range.
+__global__ void __launch_bounds__(RESORT_THREADS)
+resort_place_stayers_kernel(const unsigned* __restrict__ mask, const unsigned* __restrict__ wpre, long long n,
+                            const unsigned* __restrict__ old_keys, const unsigned* __restrict__ old_perm,
+                            const unsigned* __restrict__ mk, const unsigned* __restrict__ mp,
+                            const int* __restrict__ n_movers, unsigned* __restrict__ keys_out,
+                            unsigned* __restrict__ perm_out) {
+    __shared__ int range[2];
+    const long long q0 = (long long)blockIdx.x * RESORT_THREADS;
+    const long long q = q0 + threadIdx.x;
+    const int nm = *n_movers;
+    if (threadIdx.x < 2) {
+        const long long qe = threadIdx.x == 0 ? q0 : min(q0 + RESORT_THREADS, n) - 1;
+        const unsigned long long v = pair_key(old_keys[qe], old_perm[qe]) + (threadIdx.x == 0 ? 0ull : 1ull);
+        range[threadIdx.x] = mover_bound(mk, mp, v, 0, nm);
+    }
+    __syncthreads();
+    if (q >= n) return;
+    const unsigned m = mask[q >> 5];
+    if ((m >> (q & 31)) & 1u) return;
+    const unsigned k = old_keys[q], p = old_perm[q];
+    const int j = mover_bound(mk, mp, pair_key(k, p), range[0], range[1]);
+    const long long pos = q - (long long)resort_movers_before(mask, wpre, q, n, (unsigned)nm) + j;
+    if (MPM_INB(pos, n, 10)) {
+        keys_out[pos] = k;
+        perm_out[pos] = p;
+    }
+}
+
+// Movers to their new slots (grid-strided over the device-side count).
+__global__ void __launch_bounds__(RESORT_THREADS)
+resort_place_movers_kernel(const unsigned* __restrict__ mask, const unsigned* __restrict__ wpre, long long n,
+                           const unsigned* __restrict__ old_keys, const unsigned* __restrict__ old_perm,
+                           const unsigned* __restrict__ mk, const unsigned* __restrict__ mp,
+                           const int* __restrict__ n_movers, unsigned* __restrict__ keys_out,
+                           unsigned* __restrict__ perm_out) {
+    const int nm = *n_movers;
+    for (long long i = (long long)blockIdx.x * RESORT_THREADS + threadIdx.x; i < nm;
+         i += (long long)gridDim.x * RESORT_THREADS) {
+        const unsigned k = mk[i], p = mp[i];
+        const unsigned long long v = pair_key(k, p);
+        long long lo = 0, hi = n;   // old slots ordered before this mover (stayers among them keep their key)
+        while (lo < hi) {
+            const long long mid = (lo + hi) >> 1;
+            if (pair_key(old_keys[mid], old_perm[mid]) < v) lo = mid + 1;
+            else hi = mid;
+        }
+        const long long pos = i + lo - (long long)resort_movers_before(mask, wpre, lo, n, (unsigned)nm);
+        if (MPM_INB(pos, n, 10)) {
+            keys_out[pos] = k;
+            perm_out[pos] = p;
+        }
     }
 }
 

@@ -54,7 +54,8 @@ struct MpmPlan {
     size_t o_dense_f = 0, o_dense_b = 0;
     // incremental re-sort of chained steps (SIZE_MAX: not laid out)
     size_t o_mflag = SIZE_MAX, o_pflag = 0, o_mask = 0, o_pmask = 0, o_wpre = 0, o_rblk = 0, o_pblk = 0;
-    size_t o_mkey = 0, o_mpart = 0, o_okey = 0, o_opart = 0, o_rint = 0;
+    size_t o_mkey = 0, o_mpart = 0, o_okey = 0, o_opart = 0, o_rint = 0, o_hist1 = 0;
+    int nblk_sort1 = 1;     // blocks of the movers' radix sort (one key per thread)
     int nblk_resort = 1;
     char* chain_tape = nullptr;    // the tape whose sorted order the emitted mover flags refer to
     long long n_nodes = 0;
@@ -251,12 +252,14 @@ int launch_p2g(MpmPlan* P, int mode, const Ctx& ctx, const unsigned* perm, const
 
 // Stable LSD radix sort of kin (with payload vin, or the index when null)
 // into (kout, vout), through the alternate buffers a0 and a1 (a1 may be the
-// input's own buffers).  n_dev: sort the first *n_dev keys (a device count).
+// input's own buffers), ITEMS keys per thread over nblk blocks with the digit
+// counts in hist; n_dev (may be null): sort the first *n_dev keys.
+template <int ITEMS>
 int run_radix(MpmPlan* P, const unsigned* kin, const unsigned* vin, unsigned* kout, unsigned* vout, unsigned* a0k,
-              unsigned* a0v, unsigned* a1k, unsigned* a1v, const int* n_dev, cudaStream_t st) {
-    unsigned* hist = at<unsigned>(P, P->o_hist);
+              unsigned* a0v, unsigned* a1k, unsigned* a1v, unsigned* hist, int nblk, const int* n_dev,
+              cudaStream_t st) {
     unsigned* totals = at<unsigned>(P, P->o_totals);
-    const int nblk = P->nblk_sort;
+    const int tile = SORT_THREADS * ITEMS;
     const unsigned* ksrc = kin;
     const unsigned* vsrc = vin;
     for (int pass = 0; pass < P->passes; ++pass) {
@@ -264,10 +267,11 @@ int run_radix(MpmPlan* P, const unsigned* kin, const unsigned* vin, unsigned* ko
         const bool last = pass == P->passes - 1;
         unsigned* kdst = last ? kout : ((pass & 1) ? a1k : a0k);
         unsigned* vdst = last ? vout : ((pass & 1) ? a1v : a0v);
-        radix_hist_kernel<<<nblk, SORT_THREADS, 0, st>>>(ksrc, P->n, shift, hist, nblk, n_dev);
-        radix_rowsum_kernel<<<RADIX, 256, 0, st>>>(hist, nblk, totals, n_dev);
-        radix_rowscan_kernel<<<RADIX, 256, 0, st>>>(hist, nblk, totals, n_dev);
-        radix_scatter_kernel<<<nblk, SORT_THREADS, 0, st>>>(ksrc, vsrc, P->n, shift, hist, nblk, kdst, vdst, n_dev);
+        radix_hist_kernel<ITEMS><<<nblk, SORT_THREADS, 0, st>>>(ksrc, P->n, shift, hist, nblk, n_dev);
+        radix_rowsum_kernel<<<RADIX, 256, 0, st>>>(hist, nblk, totals, tile, n_dev);
+        radix_rowscan_kernel<<<RADIX, 256, 0, st>>>(hist, nblk, totals, tile, n_dev);
+        radix_scatter_kernel<ITEMS><<<nblk, SORT_THREADS, 0, st>>>(ksrc, vsrc, P->n, shift, hist, nblk, kdst, vdst,
+                                                                  n_dev);
         ksrc = kdst;
         vsrc = vdst;
     }
@@ -277,14 +281,15 @@ int run_radix(MpmPlan* P, const unsigned* kin, const unsigned* vin, unsigned* ko
 // stable LSD radix sort of the binning keys -> tape (skeys, perm)
 int run_sort(MpmPlan* P, const unsigned* keys, unsigned* skeys, unsigned* perm, cudaStream_t st) {
     Site site(P, MPM_K_SORT, 4 * P->passes, st);
-    return run_radix(P, keys, nullptr, skeys, perm, at<unsigned>(P, P->o_kalt0), at<unsigned>(P, P->o_valt0),
-                     at<unsigned>(P, P->o_kalt1), at<unsigned>(P, P->o_valt1), nullptr, st);
+    return run_radix<SORT_ITEMS>(P, keys, nullptr, skeys, perm, at<unsigned>(P, P->o_kalt0),
+                                 at<unsigned>(P, P->o_valt0), at<unsigned>(P, P->o_kalt1),
+                                 at<unsigned>(P, P->o_valt1), at<unsigned>(P, P->o_hist), P->nblk_sort, nullptr, st);
 }
 
 // Sorted order of a chained step from the previous step's (old_tape) and the
 // mover flags its emitting G2P wrote (sort.cuh, incremental re-sort): the
-// movers, gathered in particle order, are radix-sorted by key on their
-// device-side count and merged with the slots that kept their key.
+// movers, gathered in particle order, are radix-sorted by key on their count
+// held on the device and merged with the slots that kept their key.
 int run_resort(MpmPlan* P, const char* old_tape, char* tape, const unsigned* keys, cudaStream_t st) {
     const unsigned* ok = reinterpret_cast<const unsigned*>(old_tape + P->t_skeys);
     const unsigned* op = reinterpret_cast<const unsigned*>(old_tape + P->t_perm);
@@ -322,9 +327,10 @@ int run_resort(MpmPlan* P, const char* old_tape, char* tape, const unsigned* key
     resort_compact_kernel<<<nb, RESORT_THREADS, 0, st>>>(mask, pmask, P->n, rblk, pblk, keys, wpre, mk, mp);
     int rc = check_launch();
     if (rc) return rc;
-    // movers in particle order -> (key, particle) order; the second alternate is the input's buffers
-    rc = run_radix(P, mk, mp, sk, sp, at<unsigned>(P, P->o_kalt1), at<unsigned>(P, P->o_valt1), mk, mp, n_movers,
-                   st);
+    // movers in particle order -> (key, particle) order, in (sk, sp); one key per
+    // thread, so that the movers spread over many blocks
+    rc = run_radix<1>(P, mk, mp, sk, sp, at<unsigned>(P, P->o_kalt1), at<unsigned>(P, P->o_valt1), mk, mp,
+                      at<unsigned>(P, P->o_hist1), P->nblk_sort1, n_movers, st);
     if (rc) return rc;
     resort_place_stayers_kernel<<<grid_for(P->n, RESORT_THREADS), RESORT_THREADS, 0, st>>>(
         mask, wpre, P->n, ok, op, sk, sp, n_movers, nk, np);
@@ -587,6 +593,8 @@ int mpm_plan_create(const MpmScene* scenes, int32_t n_scenes, int32_t real_bytes
     P->o_okey = L.take(n * 4);
     P->o_opart = L.take(n * 4);
     P->o_rint = L.take(8);
+    P->nblk_sort1 = (int)((P->n + SORT_THREADS - 1) / SORT_THREADS);
+    P->o_hist1 = L.take((size_t)RADIX * P->nblk_sort1 * 4);
     P->o_tape = L.take(P->tape_bytes);
     P->ws_bytes = L.off;
     *out = P;

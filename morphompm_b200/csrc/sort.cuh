@@ -1,8 +1,5 @@
 // Deterministic, stable LSD radix sort of 32-bit cell keys with 32-bit payload
-// indices, and the incremental re-sort of a chained step.  Given n_dev, the
-// radix kernels sort the first *n_dev keys (a count formed on the device; the
-// launch is sized for n): blocks past it return and the digit scans cover the
-// blocks in use only.  No global atomics: each pass builds
+// indices, and the incremental re-sort of a chained step.  No global atomics: each pass builds
 // per-block digit counts (shared-memory counters), scans them digit-major into
 // global offsets (row totals, then per-digit row scans) and scatters every key
 // to offset + its stable rank inside the block, ranked with warp match masks.
@@ -19,25 +16,28 @@ constexpr int SORT_ITEMS = 16;                       // keys per thread per bloc
 constexpr int SORT_TILE = SORT_THREADS * SORT_ITEMS; // keys per block
 
 // Blocks of a sort over *n_dev keys (a count on the device; the grid and the
-// histogram stride are sized for nblk blocks), or nblk.
-__device__ __forceinline__ int active_blocks(int nblk, const int* __restrict__ n_dev) {
+// histogram stride are sized for nblk blocks of TILE keys), or nblk.
+__device__ __forceinline__ int active_blocks(int nblk, int tile, const int* __restrict__ n_dev) {
     if (!n_dev) return nblk;
-    const long long a = ((long long)*n_dev + SORT_TILE - 1) / SORT_TILE;
+    const long long a = ((long long)*n_dev + tile - 1) / tile;
     return (int)(a < nblk ? a : nblk);
 }
 
 // Per-block digit histogram.  hist is digit-major: hist[d * nblk + b].
+// ITEMS keys per thread; n_dev (may be null): sort the first *n_dev keys.
+template <int ITEMS>
 __global__ void __launch_bounds__(SORT_THREADS)
 radix_hist_kernel(const unsigned* __restrict__ keys, long long n, int shift, unsigned* __restrict__ hist, int nblk,
                   const int* __restrict__ n_dev) {
+    constexpr int TILE = SORT_THREADS * ITEMS;
     if (n_dev) n = *n_dev;
-    if ((long long)blockIdx.x * SORT_TILE >= n && blockIdx.x > 0) return;
+    if ((long long)blockIdx.x * TILE >= n) return;      // past a device-side count
     __shared__ unsigned cnt[RADIX];
     for (int d = threadIdx.x; d < RADIX; d += SORT_THREADS) cnt[d] = 0;
     __syncthreads();
-    long long base = (long long)blockIdx.x * SORT_TILE;
+    long long base = (long long)blockIdx.x * TILE;
 #pragma unroll 4
-    for (int r = 0; r < SORT_ITEMS; ++r) {
+    for (int r = 0; r < ITEMS; ++r) {
         long long q = base + (long long)r * SORT_THREADS + threadIdx.x;
         if (q < n) atomicAdd(&cnt[(keys[q] >> shift) & (RADIX - 1)], 1u);
     }
@@ -47,9 +47,9 @@ radix_hist_kernel(const unsigned* __restrict__ keys, long long n, int shift, uns
 
 // totals[d] = sum_b hist[d][b]   (one block per digit, fixed-order tree)
 __global__ void __launch_bounds__(256)
-radix_rowsum_kernel(const unsigned* __restrict__ hist, int nblk, unsigned* __restrict__ totals,
+radix_rowsum_kernel(const unsigned* __restrict__ hist, int nblk, unsigned* __restrict__ totals, int tile,
                     const int* __restrict__ n_dev) {
-    const int nact = active_blocks(nblk, n_dev);
+    const int nact = active_blocks(nblk, tile, n_dev);
     __shared__ unsigned red[256];
     int d = blockIdx.x;
     unsigned s = 0;
@@ -65,9 +65,9 @@ radix_rowsum_kernel(const unsigned* __restrict__ hist, int nblk, unsigned* __res
 
 // hist[d][b] <- sum_{d'<d} totals[d'] + sum_{b'<b} hist[d][b']   (one block per digit)
 __global__ void __launch_bounds__(256)
-radix_rowscan_kernel(unsigned* __restrict__ hist, int nblk, const unsigned* __restrict__ totals,
+radix_rowscan_kernel(unsigned* __restrict__ hist, int nblk, const unsigned* __restrict__ totals, int tile,
                      const int* __restrict__ n_dev) {
-    const int nact = active_blocks(nblk, n_dev);
+    const int nact = active_blocks(nblk, tile, n_dev);
     __shared__ unsigned sh[256];
     __shared__ unsigned carry;
     int d = blockIdx.x;
@@ -110,24 +110,26 @@ radix_rowscan_kernel(unsigned* __restrict__ hist, int nblk, const unsigned* __re
 // into the warps' output offsets per digit, pass 2 scatters: a key's
 // position is its warp's running offset for its digit plus its rank among the
 // lanes of its round with the same digit (warp match masks).
+template <int ITEMS>
 __global__ void __launch_bounds__(SORT_THREADS)
 radix_scatter_kernel(const unsigned* __restrict__ keys_in, const unsigned* __restrict__ vals_in, long long n,
                      int shift, const unsigned* __restrict__ offs, int nblk,
                      unsigned* __restrict__ keys_out, unsigned* __restrict__ vals_out, const int* __restrict__ n_dev) {
+    constexpr int TILE = SORT_THREADS * ITEMS;
     if (n_dev) n = *n_dev;
-    if ((long long)blockIdx.x * SORT_TILE >= n) return;
+    if ((long long)blockIdx.x * TILE >= n) return;
     constexpr int NW = SORT_THREADS / 32;
-    constexpr int PER_WARP = SORT_TILE / NW;   // SORT_ITEMS rounds of 32 keys
+    constexpr int PER_WARP = TILE / NW;   // ITEMS rounds of 32 keys
     __shared__ unsigned wcnt[NW][RADIX];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const unsigned lt_mask = (1u << lane) - 1u;
     for (int i = threadIdx.x; i < NW * RADIX; i += SORT_THREADS) (&wcnt[0][0])[i] = 0;
     __syncthreads();
-    const long long wbase = (long long)blockIdx.x * SORT_TILE + (long long)warp * PER_WARP;
-    unsigned key[SORT_ITEMS], val[SORT_ITEMS];
+    const long long wbase = (long long)blockIdx.x * TILE + (long long)warp * PER_WARP;
+    unsigned key[ITEMS], val[ITEMS];
     // pass 1: digit counts of this warp's chunk
 #pragma unroll
-    for (int r = 0; r < SORT_ITEMS; ++r) {
+    for (int r = 0; r < ITEMS; ++r) {
         const long long q = wbase + (long long)r * 32 + lane;
         const bool valid = q < n;
         key[r] = valid ? keys_in[q] : 0u;
@@ -154,7 +156,7 @@ radix_scatter_kernel(const unsigned* __restrict__ keys_in, const unsigned* __res
     __syncthreads();
     // pass 2: scatter
 #pragma unroll
-    for (int r = 0; r < SORT_ITEMS; ++r) {
+    for (int r = 0; r < ITEMS; ++r) {
         const long long q = wbase + (long long)r * 32 + lane;
         const bool valid = q < n;
         const unsigned dig = (key[r] >> shift) & (RADIX - 1);
@@ -186,7 +188,8 @@ radix_scatter_kernel(const unsigned* __restrict__ keys_in, const unsigned* __res
 // whether the particle's new key differs from its old one (a "mover").  The
 // slots that keep their key ("stayers") are still in (key, particle) order.
 // The movers are gathered in particle order and stable-sorted by key with the
-// radix sort on their device-side count, which puts them in (key, particle)
+// radix kernels on their device-side count (tiles of 256 keys, so that the few
+// thousand movers spread over many blocks), which puts them in (key, particle)
 // order; then the two sorted sequences are merged: the stayer at old slot q
 // goes to q - (movers before q) + (movers ordered before it), mover i to
 // i + (stayers ordered before it).  The result is exactly the full sort's.
@@ -310,30 +313,20 @@ __device__ __forceinline__ int mover_bound(const unsigned* __restrict__ mk, cons
     return lo;
 }
 
-// Stayers to their new slots.  The block's slots span a key range: its first
-// and last old (key, particle) values bound the movers ordered before any of
-// its stayers, so every thread searches that narrow range.
+// Stayers to their new slots.
 __global__ void __launch_bounds__(RESORT_THREADS)
 resort_place_stayers_kernel(const unsigned* __restrict__ mask, const unsigned* __restrict__ wpre, long long n,
                             const unsigned* __restrict__ old_keys, const unsigned* __restrict__ old_perm,
                             const unsigned* __restrict__ mk, const unsigned* __restrict__ mp,
                             const int* __restrict__ n_movers, unsigned* __restrict__ keys_out,
                             unsigned* __restrict__ perm_out) {
-    __shared__ int range[2];
-    const long long q0 = (long long)blockIdx.x * RESORT_THREADS;
-    const long long q = q0 + threadIdx.x;
-    const int nm = *n_movers;
-    if (threadIdx.x < 2) {
-        const long long qe = threadIdx.x == 0 ? q0 : min(q0 + RESORT_THREADS, n) - 1;
-        const unsigned long long v = pair_key(old_keys[qe], old_perm[qe]) + (threadIdx.x == 0 ? 0ull : 1ull);
-        range[threadIdx.x] = mover_bound(mk, mp, v, 0, nm);
-    }
-    __syncthreads();
+    const long long q = (long long)blockIdx.x * RESORT_THREADS + threadIdx.x;
     if (q >= n) return;
     const unsigned m = mask[q >> 5];
     if ((m >> (q & 31)) & 1u) return;
+    const int nm = *n_movers;
     const unsigned k = old_keys[q], p = old_perm[q];
-    const int j = mover_bound(mk, mp, pair_key(k, p), range[0], range[1]);
+    const int j = mover_bound(mk, mp, pair_key(k, p), 0, nm);     // movers ordered before this stayer
     const long long pos = q - (long long)resort_movers_before(mask, wpre, q, n, (unsigned)nm) + j;
     if (MPM_INB(pos, n, 10)) {
         keys_out[pos] = k;

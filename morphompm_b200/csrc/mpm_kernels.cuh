@@ -729,15 +729,18 @@ __global__ void __launch_bounds__(1024)
 node_sums_kernel(Ctx ctx, const R* __restrict__ S, long long cap, const int* __restrict__ active,
                  const int* __restrict__ n_active, R* __restrict__ grid_out, const R* __restrict__ grid_fwd,
                  int advect) {
-    // The two modes keep different loop shapes: each is the faster of those
-    // measured for its mode (config 4: forward 65.8 vs 71.9 ms, reverse 80.8
-    // vs 91.0 ms per trajectory); the sums and their order are the same.
+    // Both modes walk the nodes in CTA-uniform rounds of blockDim nodes (the
+    // per-thread grid-stride form measured slower: forward 62.3 vs 65.8 ms,
+    // reverse 80.8 vs 86.7 ms per config-4 trajectory); the forward keeps its
+    // epilogue inline and the reverse calls node_adjoint, each the faster of
+    // the two measured for its mode.  The sums and their order are the same.
     if constexpr (MODE == 0) {
         constexpr int TN = T * T * TZ;
         // one thread per node of the active tiles (tile-major, z fastest), grid-strided
         const long long total = (long long)(*n_active) * TN;
-        for (long long gidx = (long long)blockIdx.x * blockDim.x + threadIdx.x; gidx < total;
-             gidx += (long long)gridDim.x * blockDim.x) {
+        for (long long r0 = (long long)blockIdx.x * blockDim.x; r0 < total; r0 += (long long)gridDim.x * blockDim.x) {
+            const long long gidx = r0 + threadIdx.x;
+            if (gidx >= total) continue;
             const int it = (int)(gidx / TN), node = (int)(gidx % TN);
             const int tile = active[it];
             const int s = ctx.tile_scene[tile];

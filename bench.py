@@ -49,6 +49,9 @@ def parse():
     ap.add_argument("--workload", default="config4", choices=["config1", "config2", "config3", "config4", "config5"],
                     help="config4 is the headline line; the others print one line each for the other growth "
                          "workloads (FP64 and FP32 where the workload names both)")
+    ap.add_argument("--conditioning", action="store_true",
+                    help="with --workload: how far FP64 moves when only the initial positions are rounded to "
+                         "FP32, next to the FP32 error (one JSON line)")
     return ap.parse_args()
 
 
@@ -248,11 +251,11 @@ def kernel_bytes_per_particle(kind, w):
 
 
 # DRAM bytes (read + write) per particle per launch of the heaviest kernels, from
-# one `ncu --set full` capture of a 2,092,825-particle batch of the config-4
-# generator (FP32, chained steps); their traffic grows in proportion to the
-# particles, so it is scaled to the workload.
+# `ncu` captures of a 2,092,825-particle batch of the config-4 generator (FP32,
+# chained steps; profiles/reverse_particle_dram_config4_128scenes.md); their
+# traffic grows in proportion to the particles, so it is scaled to the workload.
 MEASURED_TRAFFIC_PER_PARTICLE = {
-    "bwd_particle": (526.156288e6 + 210.969088e6) / 2092825,
+    "bwd_particle": (526191872 + 212122624) / 2092825,
     "g2p": (137.490688e6 + 339.093504e6) / 2092825,
 }
 
@@ -266,6 +269,8 @@ def main():
     a = parse()
     if a.impl == "reference":
         return run_reference(a)
+    if a.conditioning:
+        return run_conditioning(a)
     if a.workload != "config4":
         return run_other(a)
     import torch
@@ -391,7 +396,8 @@ def main():
             "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
             "traffic": (MEASURED_TRAFFIC_PER_PARTICLE[dominant] * n_tot
                         if dominant in MEASURED_TRAFFIC_PER_PARTICLE else None),
-            "traffic_source": "ncu dram bytes per launch, 2.09M-particle capture scaled by particles",
+            "traffic_source": "ncu dram bytes per launch, 2.09M-particle capture scaled by particles "
+                              "(profiles/reverse_particle_dram_config4_128scenes.md)",
             "avg_launch_ms": avg_ms, "launches": nl}
     # whole step against the algorithmic bytes per particle-step fwd+adj
     # (w*(156 + 32*G_touched/n), G_touched/n ~ 0.2 at 8 particles per cell)
@@ -546,6 +552,43 @@ def workload_line(w, steps, warmup):
     line["value"] = line["results"][main_key]["value"]
     line["dtype"] = "f32" if main_key == "fp32" else "f64"
     return line
+
+
+def run_conditioning(a):
+    """Conditioning of a workload's FP32 error: FP64 from the scene's initial
+    positions, FP64 from the same positions rounded to FP32 (a perturbation of
+    rounding size and nothing else), and FP32.  When the first two differ as
+    much as FP64 and FP32 do, the FP32 error is the trajectory's amplification
+    of rounding, not an error of the FP32 path."""
+    import torch
+    from morphompm_b200 import scenes as S
+    from morphompm_b200.batch import Batch, host_slab
+    from morphompm_b200.trajectory import sqrt_schedule
+    c = getattr(S, a.workload)()
+
+    def run(cc, dt):
+        ck = cc.get("ckpt_every") or (sqrt_schedule(cc["steps"]) if a.workload == "config5" else "auto")
+        b = Batch([cc], cc["steps"], dtype=dt, ckpt_every=ck)
+        b.load(host_slab([cc], np.float64 if dt == torch.float64 else np.float32), non_blocking=False)
+        b.run()
+        torch.cuda.synchronize()
+        out = (b.final_state().double().cpu().numpy(), float(b.loss[0]), float(b.dloss_dg[0]), b.plan.status())
+        del b
+        torch.cuda.empty_cache()
+        return out
+
+    def diff(u, v):
+        return {"F": float(np.max(np.abs(u[0][15:24] - v[0][15:24]))),
+                "x": float(np.max(np.abs(u[0][0:3] - v[0][0:3]))),
+                "loss_rel": abs(u[1] - v[1]) / abs(u[1]), "dLdg_rel": abs(u[2] - v[2]) / abs(u[2])}
+    r64 = run(c, torch.float64)
+    cr = dict(c, x=c["x"].astype(np.float32).astype(np.float64))
+    r64r = run(cr, torch.float64)
+    r32 = run(c, torch.float32)
+    print(json.dumps({"workload": a.workload, "name": c["name"], "mpm_steps": c["steps"],
+                      "x0_rounding": float(np.max(np.abs(cr["x"] - c["x"]))),
+                      "fp64_vs_fp64_x0_rounded": diff(r64, r64r), "fp32_vs_fp64": diff(r64, r32),
+                      "device_status": [r64[3], r64r[3], r32[3]]}), flush=True)
 
 
 def plain_leg(scn, a, value32, peak, tuning32=None):

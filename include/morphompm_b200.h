@@ -46,7 +46,7 @@ extern "C" {
 #define MPM_K_PREPASS       4   /* stress + P2G payload                      */
 #define MPM_K_P2G           5   /* P2G scatter + grid update                 */
 #define MPM_K_G2P           6   /* G2P + advection + F update                */
-#define MPM_K_BWD_PAYLOAD   7   /* G2P-adjoint payload                       */
+#define MPM_K_BWD_PAYLOAD   7   /* reserved: no kernel of this kind (the reverse P2G forms its records) */
 #define MPM_K_BWD_P2G       8   /* gv_b scatter + grid adjoint               */
 #define MPM_K_BWD_PARTICLE  9   /* P2G adjoint + constitutive VJP            */
 #define MPM_K_REDUCE       10   /* per-scene reductions                      */

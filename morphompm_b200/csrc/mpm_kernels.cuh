@@ -512,46 +512,26 @@ __device__ __forceinline__ void store_acc(R* __restrict__ S, long long cap, int 
             }
 }
 
-// OXB = 0: three lanes per cell, lane k sums the x-offset k (the three lanes
-// read the same records, one request per warp).
+// OXB: stencil x-offsets accumulated per pass over a cell's particles (3 or 1).
 template <typename R, int MODE, int OXB>
 __global__ void __launch_bounds__(128)
 cell_sums_kernel(Ctx ctx, const unsigned* __restrict__ perm, const R* __restrict__ payload, R* __restrict__ S,
                  long long cap) {
     const int nseg = *ctx.n_seg;
-    if constexpr (OXB == 0) {
-        const long long total = 3LL * nseg;
-        for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < total;
-             g += (long long)gridDim.x * blockDim.x) {
-            const int id = (int)(g / 3), ox0 = (int)(g % 3);
-            const int first = ctx.seg_first[id], last = ctx.seg_last[id];
-            if (!(MPM_INB(first, ctx.n + 1, 11) && MPM_INB(last, ctx.n + 1, 11))) continue;
-            R acc[1][3][3][4];
-            zero_acc<R, 1>(acc);
+    for (int id = blockIdx.x * blockDim.x + threadIdx.x; id < nseg; id += gridDim.x * blockDim.x) {
+        const int first = ctx.seg_first[id], last = ctx.seg_last[id];
+        if (!(MPM_INB(first, ctx.n + 1, 11) && MPM_INB(last, ctx.n + 1, 11))) continue;
+#pragma unroll 1
+        for (int ox0 = 0; ox0 < 3; ox0 += OXB) {
+            R acc[OXB][3][3][4];
+            zero_acc<R, OXB>(acc);
             for (int q = first; q < last; ++q) {
                 R r[PAYLOAD];
                 if (!MPM_INB(perm[q], ctx.n, 9)) continue;
                 load_record(payload, perm[q], r);
-                accumulate_record<R, MODE, 1>(r, ox0, acc);
+                accumulate_record<R, MODE, OXB>(r, ox0, acc);
             }
-            store_acc<R, 1>(S, cap, id, ox0, acc);
-        }
-    } else {
-        for (int id = blockIdx.x * blockDim.x + threadIdx.x; id < nseg; id += gridDim.x * blockDim.x) {
-            const int first = ctx.seg_first[id], last = ctx.seg_last[id];
-            if (!(MPM_INB(first, ctx.n + 1, 11) && MPM_INB(last, ctx.n + 1, 11))) continue;
-#pragma unroll 1
-            for (int ox0 = 0; ox0 < 3; ox0 += OXB) {
-                R acc[OXB][3][3][4];
-                zero_acc<R, OXB>(acc);
-                for (int q = first; q < last; ++q) {
-                    R r[PAYLOAD];
-                    if (!MPM_INB(perm[q], ctx.n, 9)) continue;
-                    load_record(payload, perm[q], r);
-                    accumulate_record<R, MODE, OXB>(r, ox0, acc);
-                }
-                store_acc<R, OXB>(S, cap, id, ox0, acc);
-            }
+            store_acc<R, OXB>(S, cap, id, ox0, acc);
         }
     }
 }
@@ -646,23 +626,14 @@ __device__ __forceinline__ void adj_cell(const Ctx& ctx, const unsigned* __restr
     }
 }
 
-// OXB = 0: three lanes per cell, lane k sums the x-offset k.
+// OXB: stencil x-offsets per pass over a cell's particles (3 or 1).
 template <typename R, int OXB>
 __global__ void __launch_bounds__(128, 4)
 cell_sums_adj_kernel(Ctx ctx, const unsigned* __restrict__ perm, MpmParticles in, MpmCotangents ob,
                      R* __restrict__ S, long long cap, int advect) {
     const int nseg = *ctx.n_seg;
-    if constexpr (OXB == 0) {
-        const long long total = 3LL * nseg;
-        for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < total;
-             g += (long long)gridDim.x * blockDim.x) {
-            const int ox = (int)(g % 3);
-            adj_cell<R, 1>(ctx, perm, in, ob, S, cap, advect, (int)(g / 3), ox, ox + 1);
-        }
-    } else {
-        for (int id = blockIdx.x * blockDim.x + threadIdx.x; id < nseg; id += gridDim.x * blockDim.x)
-            adj_cell<R, OXB>(ctx, perm, in, ob, S, cap, advect, id, 0, 3);
-    }
+    for (int id = blockIdx.x * blockDim.x + threadIdx.x; id < nseg; id += gridDim.x * blockDim.x)
+        adj_cell<R, OXB>(ctx, perm, in, ob, S, cap, advect, id, 0, 3);
 }
 
 // ---------------------------------------------------------------------------

@@ -398,7 +398,9 @@ def main():
                         if dominant in MEASURED_TRAFFIC_PER_PARTICLE else None),
             "traffic_source": "ncu dram bytes per launch, 2.09M-particle capture scaled by particles "
                               "(profiles/reverse_particle_dram_config4_128scenes.md)",
-            "avg_launch_ms": avg_ms, "launches": nl}
+            "avg_launch_ms": avg_ms, "launches": nl,
+            "per_launch": "one MPM step of the kernel: its launches over every material-model run of slots "
+                          f"({len({sc['model'] for sc in scn if sc['x'].shape[0]})} per step) between one pair of CUDA events"}
     # whole step against the algorithmic bytes per particle-step fwd+adj
     # (w*(156 + 32*G_touched/n), G_touched/n ~ 0.2 at 8 particles per cell)
     step_bytes = w * (156 + 32 * 0.2) * n_tot * a.mpm_steps

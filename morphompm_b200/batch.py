@@ -84,12 +84,22 @@ class Batch:
         self.scenes = [dict(s) for s in scenes]   # set_params edits these copies
         self.n_steps = n_steps
         self.dtype = dtype
-        self.specs = [scene_spec_from_dict(s) for s in scenes]
+        # The plan holds the scenes grouped by material model (stable), so that
+        # each model's particles are one run of slots and get the kernels
+        # specialised for that model; per-scene results come back in the
+        # caller's scene order.
+        self.scene_perm = np.array(sorted(range(len(scenes)), key=lambda i: (MODEL_KIND[scenes[i]["model"]], i)),
+                                   dtype=np.int64)
+        self.specs = [scene_spec_from_dict(scenes[i]) for i in self.scene_perm]
         self.n = sum(sp.n for sp in self.specs)
         npd = np.float32 if dtype == torch.float32 else np.float64
         tuning = dict(tuning or {})
-        offsets = np.concatenate([[0], np.cumsum([sp.n for sp in self.specs])]).astype(np.int64)
-        self.order = batch_order(scenes, offsets) if reorder else None     # slot -> input particle
+        offsets = np.concatenate([[0], np.cumsum([s["x"].shape[0] for s in scenes])]).astype(np.int64)
+        # slot -> input particle
+        self.order = batch_order(scenes, offsets, self.scene_perm, cell_order=reorder)
+        self._scene_inv = None
+        if np.any(self.scene_perm != np.arange(len(scenes))):
+            self._scene_inv = torch.as_tensor(np.argsort(self.scene_perm))
         phi = host_phi(scenes, npd)
         if phi is not None and self.order is not None:
             phi = np.ascontiguousarray(phi[self.order])
@@ -119,6 +129,8 @@ class Batch:
         self.rollout = Rollout(self.plan, n_steps, advect=advect, ckpt_every=self.ckpt_every, Fg=None, loss=loss,
                                x_obs=xo, material_grads=material_grads)
         self.slab0 = torch.empty(SLAB_ROWS, self.n, dtype=dtype, device=self.plan.device)
+        if self._scene_inv is not None:
+            self._scene_inv = self._scene_inv.to(self.plan.device)
         self.order_dev = self.inverse_dev = self._stage = None
         if self.order is not None:
             dev = self.plan.device
@@ -228,24 +240,28 @@ class Batch:
             self.capture()
         self.graph.replay()
 
+    def _scene_order(self, t: torch.Tensor) -> torch.Tensor:
+        """Per-scene values of the plan (grouped by model) in the caller's scene order."""
+        return t if self._scene_inv is None else torch.index_select(t, 0, self._scene_inv)
+
     @property
     def loss(self) -> torch.Tensor:
-        return self.rollout.loss
+        return self._scene_order(self.rollout.loss)
 
     @property
     def dloss_dg(self) -> torch.Tensor:
         """d loss_s / d g_s (growth law g_s = 1 + A_s, so d/dA = d/dg)."""
-        return self.rollout.growth_grad
+        return self._scene_order(self.rollout.growth_grad)
 
     @property
     def dloss_dmaterial(self) -> torch.Tensor:
         """(S, 2): d loss_s / d mu_s, d loss_s / d lambda_s (material_grads=True)."""
-        return self.rollout.material_grad
+        return self._scene_order(self.rollout.material_grad)
 
     def dloss_dE_nu(self) -> np.ndarray:
         """(S, 2) on the host: d loss_s / d E_s, d loss_s / d nu_s."""
         from .integrate import lame_to_young
-        mg = self.rollout.material_grad.cpu().numpy()
+        mg = self.dloss_dmaterial.cpu().numpy()
         out = np.zeros_like(mg)
         for s, sc in enumerate(self.scenes):
             out[s] = lame_to_young(mg[s, 0], mg[s, 1], float(sc["E"]), float(sc["nu"]))
@@ -265,7 +281,7 @@ class Batch:
             if E is not None or nu is not None:
                 sc["mu"] = sc["E"] / (2.0 * (1.0 + sc["nu"]))
                 sc["lam"] = sc["E"] * sc["nu"] / ((1.0 + sc["nu"]) * (1.0 - 2.0 * sc["nu"]))
-        self.specs = [scene_spec_from_dict(s) for s in self.scenes]
+        self.specs = [scene_spec_from_dict(self.scenes[i]) for i in self.scene_perm]
         self.plan.update_scenes(self.specs)
 
 

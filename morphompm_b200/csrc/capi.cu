@@ -11,6 +11,7 @@
 #include <cstring>
 #include <mutex>
 #include <new>
+#include <type_traits>
 #include <vector>
 
 #include "../../include/morphompm_b200.h"
@@ -58,6 +59,11 @@ struct MpmPlan {
     int nblk_sort1 = 1;     // blocks of the movers' radix sort (one key per thread)
     int nblk_resort = 1;
     char* chain_tape = nullptr;    // the tape whose sorted order the emitted mover flags refer to
+    // runs of consecutive scenes with one material model (their slot ranges);
+    // grouped: every model has one run, so each run gets a kernel for its model
+    std::vector<int> run_kind;
+    std::vector<long long> run_begin, run_end;
+    bool runs_grouped = false;
     long long n_nodes = 0;
     size_t o_dbuf, o_tape;
     int nblk_seg = 1, nblk_tile = 1;
@@ -278,6 +284,34 @@ int run_radix(MpmPlan* P, const unsigned* kin, const unsigned* vin, unsigned* ko
     return check_launch();
 }
 
+// Calls f(model constant, first slot, end slot) once per run of scenes with
+// one material model when the plan's scenes are grouped by model (f then
+// launches the kernel specialised for that model), else once over all slots
+// with the runtime model switch (constant -1).  Returns the number of calls.
+template <typename Fn>
+int for_model_runs(const MpmPlan* P, Fn&& f) {
+    if (!P->runs_grouped) {
+        f(std::integral_constant<int, -1>{}, 0LL, P->n);
+        return 1;
+    }
+    int k = 0;
+    for (size_t r = 0; r < P->run_kind.size(); ++r) {
+        const long long b = P->run_begin[r], e = P->run_end[r];
+        switch (P->run_kind[r]) {
+            case MPM_MODEL_NEOHOOKEAN: f(std::integral_constant<int, MPM_MODEL_NEOHOOKEAN>{}, b, e); break;
+            case MPM_MODEL_HENCKY: f(std::integral_constant<int, MPM_MODEL_HENCKY>{}, b, e); break;
+            case MPM_MODEL_HERSCHEL_BULKLEY:
+                f(std::integral_constant<int, MPM_MODEL_HERSCHEL_BULKLEY>{}, b, e);
+                break;
+            default: f(std::integral_constant<int, -1>{}, b, e); break;
+        }
+        ++k;
+    }
+    return k;
+}
+
+int model_run_count(const MpmPlan* P) { return P->runs_grouped ? (int)P->run_kind.size() : 1; }
+
 // stable LSD radix sort of the binning keys -> tape (skeys, perm)
 int run_sort(MpmPlan* P, const unsigned* keys, unsigned* skeys, unsigned* perm, cudaStream_t st) {
     Site site(P, MPM_K_SORT, 4 * P->passes, st);
@@ -375,11 +409,15 @@ int step_fwd_R(MpmPlan* P, const MpmParticles& in, MpmParticles& out, int advect
     }
     if (rc) return rc;
     {
-        Site s(P, MPM_K_G2P, 1, st);
-        if (emit)
-            g2p_kernel<R, true><<<g, B, 0, st>>>(ctx, tp, in, out, advect, keys, payload, t);
-        else
-            g2p_kernel<R, false><<<g, B, 0, st>>>(ctx, tp, in, out, advect, keys, payload, t);
+        Site s(P, MPM_K_G2P, model_run_count(P), st);
+        for_model_runs(P, [&](auto kind, long long b, long long e) {
+            constexpr int K = decltype(kind)::value;
+            const int gr = grid_for(e - b, B);
+            if (emit)
+                g2p_kernel<R, true, K><<<gr, B, 0, st>>>(ctx, tp, in, out, advect, keys, payload, t, b, e);
+            else
+                g2p_kernel<R, false, K><<<gr, B, 0, st>>>(ctx, tp, in, out, advect, keys, payload, t, b, e);
+        });
     }
     return check_launch();
 }
@@ -423,14 +461,25 @@ int step_bwd_R(MpmPlan* P, const MpmParticles& in, const void* outC, const MpmCo
         const R* oC = static_cast<const R*>(outC);
         double* dAp = want_dA ? dbuf : nullptr;
         if (P->any_external) {
+            const long long n = P->n;
             if (material_grad)
-                bwd_particle_kernel<R, true, true><<<g, B, 0, st>>>(ctx, tp, in, oC, ob, ib, dAp, dmat, advect, t);
+                bwd_particle_kernel<R, true, true, -1><<<g, B, 0, st>>>(ctx, tp, in, oC, ob, ib, dAp, dmat, advect,
+                                                                        t, 0, n);
             else
-                bwd_particle_kernel<R, false, true><<<g, B, 0, st>>>(ctx, tp, in, oC, ob, ib, dAp, nullptr, advect, t);
-        } else if (material_grad) {
-            bwd_particle_kernel<R, true, false><<<g, B, 0, st>>>(ctx, tp, in, oC, ob, ib, dAp, dmat, advect, t);
+                bwd_particle_kernel<R, false, true, -1><<<g, B, 0, st>>>(ctx, tp, in, oC, ob, ib, dAp, nullptr,
+                                                                         advect, t, 0, n);
         } else {
-            bwd_particle_kernel<R, false, false><<<g, B, 0, st>>>(ctx, tp, in, oC, ob, ib, dAp, nullptr, advect, t);
+            P->launches += model_run_count(P) - 1;
+            for_model_runs(P, [&](auto kind, long long b, long long e) {
+                constexpr int K = decltype(kind)::value;
+                const int gr = grid_for(e - b, B);
+                if (material_grad)
+                    bwd_particle_kernel<R, true, false, K><<<gr, B, 0, st>>>(ctx, tp, in, oC, ob, ib, dAp, dmat,
+                                                                             advect, t, b, e);
+                else
+                    bwd_particle_kernel<R, false, false, K><<<gr, B, 0, st>>>(ctx, tp, in, oC, ob, ib, dAp, nullptr,
+                                                                              advect, t, b, e);
+            });
         }
     }
     if (want_dA) {
@@ -531,6 +580,22 @@ int mpm_plan_create(const MpmScene* scenes, int32_t n_scenes, int32_t real_bytes
         for (long long k = a.tile_begin; k < tile; ++k) P->tile_scene.push_back(s);
     }
     if (cell >= (1LL << 31) || pcur >= (1LL << 31) || pcur < 1) { delete P; return MPM_ERR_ARG; }
+    // runs of consecutive non-empty scenes with one model; grouped when no
+    // model has two runs (and no scene supplies its own stress)
+    for (const MpmScene& sc : P->scenes) {
+        if (sc.p_end == sc.p_begin) continue;
+        if (!P->run_kind.empty() && P->run_kind.back() == sc.model) {
+            P->run_end.back() = sc.p_end;
+        } else {
+            P->run_kind.push_back(sc.model);
+            P->run_begin.push_back(sc.p_begin);
+            P->run_end.push_back(sc.p_end);
+        }
+    }
+    P->runs_grouped = !P->any_external && !P->run_kind.empty();
+    for (size_t a = 0; a < P->run_kind.size(); ++a)
+        for (size_t b = a + 1; b < P->run_kind.size(); ++b)
+            if (P->run_kind[a] == P->run_kind[b]) P->runs_grouped = false;
     P->n = pcur;
     P->n_tiles = tile;
     P->n_keys = cell;

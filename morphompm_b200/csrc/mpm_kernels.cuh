@@ -379,12 +379,13 @@ seg_write_kernel(Ctx ctx, const unsigned* __restrict__ skeys) {
 // forward prepass: stress -> P2G record, stored in particle order
 // record: fx[0..2], pmass, a = pmass v, B = (pmass C + dt sk) dx
 // ---------------------------------------------------------------------------
-template <typename R>
+template <typename R, int KIND = -1>
 __device__ __forceinline__ void p2g_record(const Ctx& ctx, const MpmScene& sc, long long p, const R fx[3],
                                            const R v[3], const R C[9], const R F[9], const R Fg[9],
                                            R rec[PAYLOAD]) {
     ModelParams<R> M;
     M.load(sc);
+    if constexpr (KIND >= 0) M.kind = KIND;     // a launch over scenes of one model
     const R dx = (R)sc.dx, dt = (R)sc.dt, inv_dx = (R)(1.0 / sc.dx);
     const R k4 = R(4) * inv_dx * inv_dx;
     R tau[9];
@@ -861,12 +862,14 @@ __device__ __forceinline__ void unmark_cell(const Ctx& ctx, const SceneAux& ax, 
 // G2P + advection + F update (transfer.py:61-79); writes the output state in
 // the input's particle order and clears the cell marks of this step.
 // ---------------------------------------------------------------------------
-template <typename R, bool EMIT>
+// Sorted slots [s_begin, s_end).  KIND >= 0: every scene of these slots uses
+// material model KIND, so the kernel carries that model's code only.
+template <typename R, bool EMIT, int KIND>
 __global__ void __launch_bounds__(256, EMIT ? (sizeof(R) == 4 ? 3 : 1) : (sizeof(R) == 4 ? 4 : 2))
 g2p_kernel(Ctx ctx, Tape<R> tp, MpmParticles in, MpmParticles out, int advect, unsigned* __restrict__ keys,
-           R* __restrict__ payload, int t) {
-    long long sidx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (sidx >= ctx.n) return;
+           R* __restrict__ payload, int t, long long s_begin, long long s_end) {
+    long long sidx = s_begin + (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (sidx >= s_end) return;
     long long p = tp.perm[sidx];
     if (!MPM_INB(p, ctx.n, 9)) return;
     const int s = ctx.scene_of[sidx];
@@ -957,7 +960,7 @@ g2p_kernel(Ctx ctx, Tape<R> tp, MpmParticles in, MpmParticles out, int advect, u
             ctx.mover_pflag[p] = moved;
         }
         load_Fg<R>(ctx, sc, in, p, t + 1, Fg, nullptr);
-        p2g_record<R>(ctx, sc, p, fxn, nv, nC, Fn, Fg, rec);
+        p2g_record<R, KIND>(ctx, sc, p, fxn, nv, nC, Fn, Fg, rec);
         store_record(payload, p, rec);
     }
 }
@@ -971,13 +974,14 @@ g2p_kernel(Ctx ctx, Tape<R> tp, MpmParticles in, MpmParticles out, int advect, u
 // ---------------------------------------------------------------------------
 // MAT: also the material-parameter gradients per slot, dmat[sidx] (mu) and
 // dmat[n + sidx] (lambda).  EXT: the plan has MPM_MODEL_EXTERNAL scenes.
-template <typename R, bool MAT, bool EXT>
+// Sorted slots [s_begin, s_end); KIND as in g2p_kernel.
+template <typename R, bool MAT, bool EXT, int KIND>
 __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 2 : 1)
 bwd_particle_kernel(Ctx ctx, Tape<R> tp, MpmParticles in, const R* __restrict__ outC,
                     MpmCotangents ob, MpmCotangents ib, double* __restrict__ dA, double* __restrict__ dmat,
-                    int advect, int t) {
-    long long sidx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (sidx >= ctx.n) return;
+                    int advect, int t, long long s_begin, long long s_end) {
+    long long sidx = s_begin + (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (sidx >= s_end) return;
     long long p = tp.perm[sidx];
     if (!MPM_INB(p, ctx.n, 9)) return;
     const int s = ctx.scene_of[sidx];
@@ -985,6 +989,7 @@ bwd_particle_kernel(Ctx ctx, Tape<R> tp, MpmParticles in, const R* __restrict__ 
     const SceneAux& ax = ctx.aux[s];
     ModelParams<R> M;
     M.load(sc);
+    if constexpr (KIND >= 0) M.kind = KIND;
     const R dx = (R)sc.dx, dt = (R)sc.dt, inv_dx = (R)(1.0 / sc.dx);
     const R k4 = R(4) * inv_dx * inv_dx;
     R pm, vol0;

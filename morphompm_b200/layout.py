@@ -52,18 +52,25 @@ def cell_order_device(x: torch.Tensor, dx: float, shape: Sequence[int]) -> Optio
     return torch.argsort(key, stable=True)
 
 
-def batch_order(scenes, offsets: Sequence[int]) -> Optional[np.ndarray]:
-    """Batch-wide permutation (slot -> input particle index) that puts each
-    scene's particles in cell order within its own range; None when every
-    scene already is."""
-    order = np.arange(int(offsets[-1]), dtype=np.int64)
-    changed = False
-    for s, p0 in zip(scenes, offsets[:-1]):
-        k = s["x"].shape[0]
-        if k < 2:
-            continue
-        o = cell_order_host(s["x"], float(s["dx"]), s["shape"])
-        if np.any(o != np.arange(k)):
-            order[p0:p0 + k] = p0 + o
-            changed = True
+def batch_order(scenes, offsets: Sequence[int], scene_perm: Optional[Sequence[int]] = None,
+                cell_order: bool = True) -> Optional[np.ndarray]:
+    """Batch-wide permutation (slot -> input particle index).  The input holds
+    the scenes in their given order, scene s at offsets[s]; the slots hold
+    them in the order scene_perm (default: the given order), and each scene's
+    particles in cell order within its range (cell_order).  None when that is
+    the identity."""
+    n = int(offsets[-1])
+    perm = list(range(len(scenes))) if scene_perm is None else [int(i) for i in scene_perm]
+    order = np.empty(n, dtype=np.int64)
+    changed = perm != list(range(len(scenes)))
+    q = 0
+    for s in perm:
+        sc, p0 = scenes[s], int(offsets[s])
+        k = sc["x"].shape[0]
+        o = np.arange(k)
+        if cell_order and k >= 2:
+            o = cell_order_host(sc["x"], float(sc["dx"]), sc["shape"])
+            changed = changed or bool(np.any(o != np.arange(k)))
+        order[q:q + k] = p0 + o
+        q += k
     return order if changed else None

@@ -255,7 +255,8 @@ def kernel_bytes_per_particle(kind, w):
 # chained steps; profiles/reverse_particle_dram_config4_128scenes.md); their
 # traffic grows in proportion to the particles, so it is scaled to the workload.
 MEASURED_TRAFFIC_PER_PARTICLE = {
-    "bwd_particle": (526191872 + 212122624) / 2092825,
+    # the neo-Hookean and the Hencky run of one reverse step (the kernel specialised per model)
+    "bwd_particle": (281422336 + 91672832 + 244270848 + 82131456) / 2092825,
     "g2p": (137.490688e6 + 339.093504e6) / 2092825,
 }
 

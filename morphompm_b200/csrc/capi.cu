@@ -366,8 +366,8 @@ int run_resort(MpmPlan* P, const char* old_tape, char* tape, const unsigned* key
     rc = run_radix<1>(P, mk, mp, sk, sp, at<unsigned>(P, P->o_kalt1), at<unsigned>(P, P->o_valt1), mk, mp,
                       at<unsigned>(P, P->o_hist1), P->nblk_sort1, n_movers, st);
     if (rc) return rc;
-    resort_place_stayers_kernel<<<grid_for(P->n, RESORT_THREADS), RESORT_THREADS, 0, st>>>(
-        mask, wpre, P->n, ok, op, sk, sp, n_movers, nk, np);
+    const int gs = grid_for(P->n, (RESORT_THREADS / 32) * 32 * STAY_ROUNDS);    // a warp per 256 slots
+    resort_place_stayers_kernel<<<gs, RESORT_THREADS, 0, st>>>(mask, wpre, P->n, ok, op, sk, sp, n_movers, nk, np);
     const int gm = (int)std::max<long long>(1, std::min<long long>(grid_for(P->n, RESORT_THREADS), (long long)P->n_sm * 8));
     resort_place_movers_kernel<<<gm, RESORT_THREADS, 0, st>>>(mask, wpre, P->n, ok, op, sk, sp, n_movers, nk, np);
     return check_launch();

@@ -6,9 +6,10 @@
 //   Herschel-Bulkley   python/morphompm/constitutive.py:106-147
 //
 // Morphoelastic kinematics Fe = F Fg^{-1}.  Hencky is evaluated as an
-// isotropic function of b = Fe Fe^T through a symmetric 3x3 eigensolve
-// (cyclic Jacobi rotations, Rutishauser's update), which is equivalent to the
-// reference's SVD form tau = U diag(2 mu ln s + lam sum ln s) U^T since b = U S^2 U^T.
+// isotropic function of b = Fe Fe^T through a symmetric 3x3 eigensolve (FP64:
+// cyclic Jacobi rotations, Rutishauser's update; FP32: closed form from the
+// characteristic cubic), which is equivalent to the reference's SVD form
+// tau = U diag(2 mu ln s + lam sum ln s) U^T since b = U S^2 U^T.
 #pragma once
 
 #include "mpm_common.cuh"
@@ -97,6 +98,88 @@ __device__ __forceinline__ void sym_eig3(const R S[9], R lam[3], R V[9]) {
     lam[2] = A[2][2];
 }
 
+// FP32 symmetric 3x3 eigensolve in closed form, no iteration (the trigonometric
+// solution of the characteristic cubic; Smith, "Eigenvalues of a symmetric 3x3
+// matrix", CACM 4(4), 1961):
+//   m = tr(A)/3, p = sqrt(|A - mI|_F^2 / 6), r = det((A - mI)/p)/2,
+//   phi = acos(r)/3, lambda = m + 2p cos(phi + 2k pi/3).
+// The eigenvector of the eigenvalue farthest from the other two is the largest
+// cross product of two rows of A - lambda I (well conditioned: its gap is at
+// least half the spread).  The other two come from one Jacobi rotation of A
+// restricted to the orthogonal complement of that vector, and all three
+// eigenvalues are then Rayleigh quotients, accurate to FP32 rounding of |A|
+// also when two of them are close (the cubic's roots are not, there).
+// Columns of V are the eigenvectors, V[3k + j] = component k of vector j.
+__device__ __forceinline__ void sym_eig3_closed(const float S[9], float lam[3], float V[9]) {
+    const float a00 = S[0], a11 = S[4], a22 = S[8];
+    const float a01 = 0.5f * (S[1] + S[3]), a02 = 0.5f * (S[2] + S[6]), a12 = 0.5f * (S[5] + S[7]);
+    const float m = (a00 + a11 + a22) * (1.0f / 3.0f);
+    const float b00 = a00 - m, b11 = a11 - m, b22 = a22 - m;
+    const float p2 = (b00 * b00 + b11 * b11 + b22 * b22 + 2.0f * (a01 * a01 + a02 * a02 + a12 * a12)) * (1.0f / 6.0f);
+    if (!(p2 > 1e-15f * m * m)) {
+        // spread below FP32 resolution of the trace: the diagonal is the spectrum
+        lam[0] = a00; lam[1] = a11; lam[2] = a22;
+#pragma unroll
+        for (int i = 0; i < 9; ++i) V[i] = (i % 4 == 0) ? 1.0f : 0.0f;
+        return;
+    }
+    const float ip = rsqrtf(p2), p = p2 * ip;
+    const float c00 = b00 * ip, c11 = b11 * ip, c22 = b22 * ip, c01 = a01 * ip, c02 = a02 * ip, c12 = a12 * ip;
+    float r = 0.5f * (c00 * (c11 * c22 - c12 * c12) - c01 * (c01 * c22 - c12 * c02) + c02 * (c01 * c12 - c11 * c02));
+    r = fminf(1.0f, fmaxf(-1.0f, r));
+    float sp, cp;
+    sincosf(acosf(r) * (1.0f / 3.0f), &sp, &cp);
+    const float l0 = m + 2.0f * p * cp;                                   // largest
+    const float l2 = m - p * (cp + 1.7320508075688772f * sp);             // smallest: cos(phi + 2pi/3)
+    const float l1 = 3.0f * m - l0 - l2;
+    const float le = (l0 - l1) >= (l1 - l2) ? l0 : l2;
+    // rows of A - le I; eigenvector = largest cross product of two rows
+    const float r00 = a00 - le, r11 = a11 - le, r22 = a22 - le;
+    float x0 = a01 * a12 - a02 * r11, x1 = a02 * a01 - r00 * a12, x2 = r00 * r11 - a01 * a01;   // row0 x row1
+    float y0 = a01 * r22 - a02 * a12, y1 = a02 * a02 - r00 * r22, y2 = r00 * a12 - a01 * a02;   // row0 x row2
+    float z0 = r11 * r22 - a12 * a12, z1 = a12 * a02 - a01 * r22, z2 = a01 * a12 - r11 * a02;   // row1 x row2
+    float nx = x0 * x0 + x1 * x1 + x2 * x2, ny = y0 * y0 + y1 * y1 + y2 * y2, nz = z0 * z0 + z1 * z1 + z2 * z2;
+    if (ny > nx) { x0 = y0; x1 = y1; x2 = y2; nx = ny; }
+    if (nz > nx) { x0 = z0; x1 = z1; x2 = z2; nx = nz; }
+    float v0 = 1.0f, v1 = 0.0f, v2 = 0.0f;
+    if (nx > 0.0f) {
+        const float in = rsqrtf(nx);
+        v0 = x0 * in; v1 = x1 * in; v2 = x2 * in;
+    }
+    // orthonormal complement u, w of v
+    float u0, u1, u2;
+    if (fabsf(v0) > fabsf(v1)) {
+        const float in = rsqrtf(v0 * v0 + v2 * v2);
+        u0 = -v2 * in; u1 = 0.0f; u2 = v0 * in;
+    } else {
+        const float in = rsqrtf(v1 * v1 + v2 * v2);
+        u0 = 0.0f; u1 = v2 * in; u2 = -v1 * in;
+    }
+    const float w0 = v1 * u2 - v2 * u1, w1 = v2 * u0 - v0 * u2, w2 = v0 * u1 - v1 * u0;
+    // A restricted to span(u, w): [[a, b], [b, c]]
+    const float Au0 = a00 * u0 + a01 * u1 + a02 * u2, Au1 = a01 * u0 + a11 * u1 + a12 * u2,
+                Au2 = a02 * u0 + a12 * u1 + a22 * u2;
+    const float Aw0 = a00 * w0 + a01 * w1 + a02 * w2, Aw1 = a01 * w0 + a11 * w1 + a12 * w2,
+                Aw2 = a02 * w0 + a12 * w1 + a22 * w2;
+    const float Av0 = a00 * v0 + a01 * v1 + a02 * v2, Av1 = a01 * v0 + a11 * v1 + a12 * v2,
+                Av2 = a02 * v0 + a12 * v1 + a22 * v2;
+    const float ra = u0 * Au0 + u1 * Au1 + u2 * Au2;
+    const float rb = u0 * Aw0 + u1 * Aw1 + u2 * Aw2;
+    const float rc = w0 * Aw0 + w1 * Aw1 + w2 * Aw2;
+    float t = 0.0f;
+    if (rb != 0.0f) {
+        const float th = (rc - ra) / (2.0f * rb);
+        t = copysignf(1.0f, th) / (fabsf(th) + sqrtf(th * th + 1.0f));
+    }
+    const float cs = rsqrtf(t * t + 1.0f), sn = t * cs;
+    lam[0] = v0 * Av0 + v1 * Av1 + v2 * Av2;
+    lam[1] = ra - t * rb;
+    lam[2] = rc + t * rb;
+    V[0] = v0; V[3] = v1; V[6] = v2;
+    V[1] = cs * u0 - sn * w0; V[4] = cs * u1 - sn * w1; V[7] = cs * u2 - sn * w2;
+    V[2] = sn * u0 + cs * w0; V[5] = sn * u1 + cs * w1; V[8] = sn * u2 + cs * w2;
+}
+
 // Model parameters in the arithmetic type of the path.
 template <typename R>
 struct ModelParams {
@@ -170,7 +253,11 @@ __device__ __forceinline__ void hencky_eig(const R F[9], const R Fg[9], R Fgi[9]
     mm(F, Fgi, Fe);
     R b[9];
     mmT(Fe, Fe, b);
-    sym_eig3(b, beta, V);
+    if constexpr (sizeof(R) == 4) {
+        sym_eig3_closed(b, beta, V);      // FP32: closed form
+    } else {
+        sym_eig3(b, beta, V);             // FP64: Jacobi sweeps to full precision
+    }
 }
 
 template <typename R>
@@ -394,6 +481,24 @@ __device__ __forceinline__ void hb_vjp(const R F[9], const R Fg[9], const R C[9]
 }
 
 // ---------------------------------------------------------------------------
+// Out-of-line Hencky evaluations.  An out-of-line call passes its arrays
+// through the local-memory stack, so the FP32 eigensolves stay inline; the
+// stand-alone Hencky VJP and the rare FP64 recompute of the stress in the
+// forward kernels go through these so that their register demand does not
+// inflate the allocation of the kernels that fuse them.  (The reverse kernel's
+// kept-eigensystem pair below inlines its FP64 branch: out of line it has no
+// spills but runs 4% slower.)
+// ---------------------------------------------------------------------------
+template <typename R>
+__device__ __noinline__ bool hencky_stress_ool(const R* F, const R* Fg, R mu, R lam, float thresh, R* tau) {
+    return Hencky<R>::stress(F, Fg, mu, lam, thresh, tau);
+}
+template <typename R>
+__device__ __noinline__ bool hencky_vjp_ool(const R* F, const R* Fg, R mu, R lam, float thresh, const R* tb, R* Fb,
+                                            R* Fgb) {
+    return Hencky<R>::vjp(F, Fg, mu, lam, thresh, tb, Fb, Fgb);
+}
+// ---------------------------------------------------------------------------
 // Hencky with the eigendecomposition kept between the stress (before the P2G
 // adjoint gather) and the VJP (after it): one eigensolve per particle in the
 // reverse kernel.  keep = {beta[3], V[9], flag}; flag 1 means the FP32 stress
@@ -435,20 +540,9 @@ __device__ __forceinline__ bool hencky_vjp_keep(const R* F, const R* Fg, R mu, R
 
 // ---------------------------------------------------------------------------
 // model dispatch.  Returns true when an FP32 Hencky evaluation went to FP64.
-// The eigensolves are inlined (an out-of-line call passes its arrays through
-// the local-memory stack); the stand-alone Hencky VJP and the rare FP64
-// recompute of the stress stay out of line so that their register demand does
-// not inflate the allocation of the kernels that fuse them.
+// The FP32 eigensolves are inlined; the out-of-line wrappers above carry the
+// stand-alone Hencky VJP and the rare FP64 recomputes.
 // ---------------------------------------------------------------------------
-template <typename R>
-__device__ __noinline__ bool hencky_stress_ool(const R* F, const R* Fg, R mu, R lam, float thresh, R* tau) {
-    return Hencky<R>::stress(F, Fg, mu, lam, thresh, tau);
-}
-template <typename R>
-__device__ __noinline__ bool hencky_vjp_ool(const R* F, const R* Fg, R mu, R lam, float thresh, const R* tb, R* Fb,
-                                            R* Fgb) {
-    return Hencky<R>::vjp(F, Fg, mu, lam, thresh, tb, Fb, Fgb);
-}
 template <typename R>
 __device__ __forceinline__ bool model_stress(const ModelParams<R>& P, float thresh, const R F[9], const R Fg[9],
                                              const R C[9], R tau[9]) {

@@ -227,33 +227,48 @@ seg_count_kernel(Ctx ctx, const unsigned* __restrict__ skeys) {
     }
 }
 
-// exclusive scan of per-block counts in place (single block); the total,
-// clamped to cap, goes to *total (a total above cap raises MPM_ERR_ARG)
+// exclusive scan of per-block counts in place (single block of 1024 threads);
+// the total, clamped to cap, goes to *total (a total above cap raises
+// MPM_ERR_ARG).  Each thread sums a run of consecutive counts, the runs are
+// scanned by warp shuffles and one pass over the 32 warp sums.
 __global__ void __launch_bounds__(1024)
 scan_counts_kernel(unsigned* __restrict__ cnt, int nblk, int* __restrict__ total, int cap, int* __restrict__ status) {
-    __shared__ unsigned sh[1024];
-    __shared__ unsigned carry;
-    if (threadIdx.x == 0) carry = 0;
-    __syncthreads();
-    for (int b0 = 0; b0 < nblk; b0 += 1024) {
-        int b = b0 + threadIdx.x;
-        unsigned v = b < nblk ? cnt[b] : 0u;
-        sh[threadIdx.x] = v;
-        __syncthreads();
-        for (int o = 1; o < 1024; o <<= 1) {
-            unsigned t = threadIdx.x >= (unsigned)o ? sh[threadIdx.x - o] : 0u;
-            __syncthreads();
-            sh[threadIdx.x] += t;
-            __syncthreads();
-        }
-        unsigned c = carry;
-        if (b < nblk) cnt[b] = c + sh[threadIdx.x] - v;
-        __syncthreads();
-        if (threadIdx.x == 1023) carry = c + sh[1023];
-        __syncthreads();
+    __shared__ unsigned wsum[32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int per = (nblk + 1023) / 1024;
+    const long long b0 = (long long)threadIdx.x * per;
+    unsigned loc = 0;
+    for (int j = 0; j < per; ++j)
+        if (b0 + j < nblk) loc += cnt[b0 + j];
+    unsigned inc = loc;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned t = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += t;
     }
-    if (threadIdx.x == 0) {
-        unsigned c = carry;
+    if (lane == 31) wsum[warp] = inc;
+    __syncthreads();
+    if (warp == 0) {
+        const unsigned w = wsum[lane];
+        unsigned wi = w;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned t = __shfl_up_sync(0xffffffffu, wi, o);
+            if (lane >= o) wi += t;
+        }
+        wsum[lane] = wi - w;
+    }
+    __syncthreads();
+    unsigned run = wsum[warp] + inc - loc;
+    for (int j = 0; j < per; ++j) {
+        if (b0 + j < nblk) {
+            const unsigned v = cnt[b0 + j];
+            cnt[b0 + j] = run;
+            run += v;
+        }
+    }
+    if (threadIdx.x == 1023) {       // its run ends at the grand total
+        unsigned c = run;
         if (c > (unsigned)cap) {
             raise_status(status, MPM_ERR_ARG);
             c = (unsigned)cap;
@@ -275,20 +290,51 @@ remark_cells_kernel(Ctx ctx, const unsigned* __restrict__ skeys) {
     }
 }
 
-// Active-tile list: the tiles flagged by the segment count pass, in tile
-// order.  Per-block counts (warp-striped, coalesced), the block scan above,
-// then ranks from warp ballots; the flags are reset for the next step.
+// exclusive scan, in place, of the block's SEG_ITEMS x 8 (round, warp) counts
+// (round-major, 128 entries, four per lane of warp 0); call from all threads
+__device__ __forceinline__ void scan_round_warp_counts(unsigned* pre) {
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    if ((threadIdx.x >> 5) == 0) {
+        unsigned v[4], tot = 0;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) { v[j] = pre[4 * lane + j]; tot += v[j]; }
+        unsigned inc = tot;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned t = __shfl_up_sync(0xffffffffu, inc, o);
+            if (lane >= o) inc += t;
+        }
+        unsigned ex = inc - tot;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) { pre[4 * lane + j] = ex; ex += v[j]; }
+    }
+    __syncthreads();
+}
+
+// Active-tile list: the flagged tiles, in tile order.  Per-block counts, the
+// block scan above, then ranks from warp ballots; the flags are reset for the
+// next step.  A block covers SEG_ITEMS warp-striped rounds of tiles (every load
+// coalesced), and all its flag loads are issued before any is used; one scan
+// of the (round, warp) counts replaces a barrier pair per round.
+// Bit r: tile base + r*256 + thread is flagged.
+__device__ __forceinline__ unsigned tile_flags(const int* __restrict__ flag, long long n_tiles, long long base) {
+    unsigned on = 0;
+    int f[SEG_ITEMS];
+#pragma unroll
+    for (int r = 0; r < SEG_ITEMS; ++r) {
+        const long long t = base + (long long)r * SEG_THREADS + threadIdx.x;
+        f[r] = t < n_tiles ? flag[t] : 0;
+    }
+#pragma unroll
+    for (int r = 0; r < SEG_ITEMS; ++r) on |= (f[r] != 0 ? 1u : 0u) << r;
+    return on;
+}
+
 __global__ void __launch_bounds__(SEG_THREADS)
 tile_count_kernel(const int* __restrict__ flag, long long n_tiles, unsigned* __restrict__ blk) {
     __shared__ unsigned red[SEG_THREADS / 32];
-    const long long base = (long long)blockIdx.x * SEG_TILE;
-    unsigned cnt = 0;
-#pragma unroll 4
-    for (int r = 0; r < SEG_ITEMS; ++r) {
-        const long long t = base + (long long)r * SEG_THREADS + threadIdx.x;
-        if (t >= n_tiles) break;
-        cnt += flag[t] ? 1u : 0u;
-    }
+    unsigned cnt = __popc(tile_flags(flag, n_tiles, (long long)blockIdx.x * SEG_TILE));
     for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
     if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = cnt;
     __syncthreads();
@@ -303,31 +349,29 @@ __global__ void __launch_bounds__(SEG_THREADS)
 tile_write_kernel(int* __restrict__ flag, long long n_tiles, const unsigned* __restrict__ blk,
                   int* __restrict__ active, int cap) {
     constexpr int NW = SEG_THREADS / 32;
-    __shared__ unsigned wtot[NW];
+    static_assert(SEG_ITEMS * NW == 128, "four (round, warp) counts per lane of the scanning warp");
+    __shared__ unsigned pre[SEG_ITEMS * NW];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const unsigned lt = (1u << lane) - 1u;
     const long long base = (long long)blockIdx.x * SEG_TILE;
-    unsigned run = blk[blockIdx.x];
+    const unsigned on = tile_flags(flag, n_tiles, base);
+#pragma unroll
+    for (int r = 0; r < SEG_ITEMS; ++r) {
+        const unsigned ball = __ballot_sync(0xffffffffu, (on >> r) & 1u);
+        if (lane == 0) pre[r * NW + warp] = __popc(ball);
+    }
+    scan_round_warp_counts(pre);
+    const unsigned run = blk[blockIdx.x];
+#pragma unroll
     for (int r = 0; r < SEG_ITEMS; ++r) {
         const long long t = base + (long long)r * SEG_THREADS + threadIdx.x;
-        const bool on = t < n_tiles && flag[t] != 0;
-        const unsigned ball = __ballot_sync(0xffffffffu, on);
-        if (lane == 0) wtot[warp] = __popc(ball);
-        __syncthreads();
-        unsigned before = run, round = 0;
-#pragma unroll
-        for (int w = 0; w < NW; ++w) {
-            const unsigned c = wtot[w];
-            if (w < warp) before += c;
-            round += c;
-        }
-        before += __popc(ball & lt);
-        if (on) {
+        const bool a = (on >> r) & 1u;
+        const unsigned ball = __ballot_sync(0xffffffffu, a);
+        if (a) {
+            const unsigned before = run + pre[r * NW + warp] + __popc(ball & lt);
             if (before < (unsigned)cap) active[before] = (int)t;
             flag[t] = 0;
         }
-        run += round;
-        __syncthreads();
     }
 }
 

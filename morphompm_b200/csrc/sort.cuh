@@ -313,28 +313,80 @@ __device__ __forceinline__ int mover_bound(const unsigned* __restrict__ mk, cons
     return lo;
 }
 
-// Stayers to their new slots.
+// First index in [lo, hi) whose pair (keys[i], vals[i]) is not ordered before
+// v, or hi: a 32-ary search by the whole warp (v, lo, hi warp-uniform).  Each
+// step probes 32 evenly spaced indices and keeps the interval between the last
+// probe ordered before v and the first one not, so about log_33 of the range
+// dependent loads instead of log_2.
+__device__ __forceinline__ long long warp_pair_bound(const unsigned* __restrict__ keys,
+                                                     const unsigned* __restrict__ vals, unsigned long long v,
+                                                     long long lo, long long hi) {
+    const int lane = threadIdx.x & 31;
+    while (hi - lo > 32) {
+        const long long span = hi - lo;
+        const long long idx = lo + ((long long)(lane + 1) * span) / 33;      // in [lo, hi) since span >= 33
+        const bool before = pair_key(keys[idx], vals[idx]) < v;
+        const int c = __popc(__ballot_sync(0xffffffffu, before));           // a prefix of the lanes
+        const long long nlo = c > 0 ? lo + ((long long)c * span) / 33 + 1 : lo;
+        const long long nhi = c < 32 ? lo + ((long long)(c + 1) * span) / 33 : hi;
+        lo = nlo;
+        hi = nhi;
+    }
+    const long long idx = lo + lane;
+    const bool before = idx < hi && pair_key(keys[idx], vals[idx]) < v;
+    return lo + __popc(__ballot_sync(0xffffffffu, before));
+}
+
+// Stayers to their new slots, one warp per STAY_ROUNDS x 32 consecutive old
+// slots.  A stayer's new slot is its old slot, minus the movers before it in
+// the old order, plus the sorted movers ordered before it.  The latter are
+// bracketed once per warp (the warp's first and last slot; the old order is
+// sorted, so every stayer of the warp lies between); inside the bracket, a few
+// movers on average, each stayer finds its own count by a short search.
+constexpr int STAY_ROUNDS = 8;
 __global__ void __launch_bounds__(RESORT_THREADS)
 resort_place_stayers_kernel(const unsigned* __restrict__ mask, const unsigned* __restrict__ wpre, long long n,
                             const unsigned* __restrict__ old_keys, const unsigned* __restrict__ old_perm,
                             const unsigned* __restrict__ mk, const unsigned* __restrict__ mp,
                             const int* __restrict__ n_movers, unsigned* __restrict__ keys_out,
                             unsigned* __restrict__ perm_out) {
-    const long long q = (long long)blockIdx.x * RESORT_THREADS + threadIdx.x;
-    if (q >= n) return;
-    const unsigned m = mask[q >> 5];
-    if ((m >> (q & 31)) & 1u) return;
+    const int lane = threadIdx.x & 31;
+    const long long c0 = ((long long)blockIdx.x * (RESORT_THREADS / 32) + (threadIdx.x >> 5)) * (32 * STAY_ROUNDS);
+    if (c0 >= n) return;                                      // warp-uniform
+    const long long cl = (c0 + 32 * STAY_ROUNDS < n ? c0 + 32 * STAY_ROUNDS : n) - 1;   // last slot of the warp
     const int nm = *n_movers;
-    const unsigned k = old_keys[q], p = old_perm[q];
-    const int j = mover_bound(mk, mp, pair_key(k, p), 0, nm);     // movers ordered before this stayer
-    const long long pos = q - (long long)resort_movers_before(mask, wpre, q, n, (unsigned)nm) + j;
-    if (MPM_INB(pos, n, 10)) {
-        keys_out[pos] = k;
-        perm_out[pos] = p;
+    unsigned k[STAY_ROUNDS], pv[STAY_ROUNDS], mw[STAY_ROUNDS], wp[STAY_ROUNDS];
+#pragma unroll
+    for (int r = 0; r < STAY_ROUNDS; ++r) {
+        const long long q = c0 + r * 32 + lane;
+        const bool valid = q < n;
+        k[r] = valid ? old_keys[q] : 0u;
+        pv[r] = valid ? old_perm[q] : 0u;
+        const long long w = (c0 >> 5) + r;                  // the round's mask word (c0 is a multiple of 32)
+        const bool wv = (w << 5) < n;
+        mw[r] = wv ? mask[w] : 0xffffffffu;
+        wp[r] = wv ? wpre[w] : 0u;
+    }
+    const unsigned long long v_first = pair_key(__shfl_sync(0xffffffffu, k[0], 0), __shfl_sync(0xffffffffu, pv[0], 0));
+    const unsigned long long v_last = pair_key(old_keys[cl], old_perm[cl]);
+    const int j_lo = (int)warp_pair_bound(mk, mp, v_first, 0, nm);
+    const int j_hi = (int)warp_pair_bound(mk, mp, v_last, j_lo, nm);
+    const unsigned lt = (1u << lane) - 1u;
+#pragma unroll
+    for (int r = 0; r < STAY_ROUNDS; ++r) {
+        const long long q = c0 + r * 32 + lane;
+        if (q >= n || ((mw[r] >> lane) & 1u)) continue;
+        const int j = mover_bound(mk, mp, pair_key(k[r], pv[r]), j_lo, j_hi);
+        const long long pos = q - (long long)(wp[r] + __popc(mw[r] & lt)) + j;
+        if (MPM_INB(pos, n, 10)) {
+            keys_out[pos] = k[r];
+            perm_out[pos] = pv[r];
+        }
     }
 }
 
-// Movers to their new slots (grid-strided over the device-side count).
+// Movers to their new slots: one mover per warp at a time, its count of old
+// slots ordered before it by the warp's 32-ary search.
 __global__ void __launch_bounds__(RESORT_THREADS)
 resort_place_movers_kernel(const unsigned* __restrict__ mask, const unsigned* __restrict__ wpre, long long n,
                            const unsigned* __restrict__ old_keys, const unsigned* __restrict__ old_perm,
@@ -342,20 +394,16 @@ resort_place_movers_kernel(const unsigned* __restrict__ mask, const unsigned* __
                            const int* __restrict__ n_movers, unsigned* __restrict__ keys_out,
                            unsigned* __restrict__ perm_out) {
     const int nm = *n_movers;
-    for (long long i = (long long)blockIdx.x * RESORT_THREADS + threadIdx.x; i < nm;
-         i += (long long)gridDim.x * RESORT_THREADS) {
+    const long long warps = (long long)gridDim.x * (RESORT_THREADS / 32);
+    for (long long i = (long long)blockIdx.x * (RESORT_THREADS / 32) + (threadIdx.x >> 5); i < nm; i += warps) {
         const unsigned k = mk[i], p = mp[i];
-        const unsigned long long v = pair_key(k, p);
-        long long lo = 0, hi = n;   // old slots ordered before this mover (stayers among them keep their key)
-        while (lo < hi) {
-            const long long mid = (lo + hi) >> 1;
-            if (pair_key(old_keys[mid], old_perm[mid]) < v) lo = mid + 1;
-            else hi = mid;
-        }
-        const long long pos = i + lo - (long long)resort_movers_before(mask, wpre, lo, n, (unsigned)nm);
-        if (MPM_INB(pos, n, 10)) {
-            keys_out[pos] = k;
-            perm_out[pos] = p;
+        const long long lo = warp_pair_bound(old_keys, old_perm, pair_key(k, p), 0, n);
+        if ((threadIdx.x & 31) == 0) {
+            const long long pos = i + lo - (long long)resort_movers_before(mask, wpre, lo, n, (unsigned)nm);
+            if (MPM_INB(pos, n, 10)) {
+                keys_out[pos] = k;
+                perm_out[pos] = p;
+            }
         }
     }
 }

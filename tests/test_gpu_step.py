@@ -56,6 +56,67 @@ def test_constitutive_fp32(golden, name):
     assert rel(Fgb, d[f"{name}_Fg_bar"]) < 5e-5
 
 
+def _spectra_cases(rng):
+    """Deformations F = Q diag(s) R^T with chosen singular values s (random
+    rotations Q, R) and growth Fg = g I: the FP32 Hencky eigensolve's hard cases."""
+    def rot():
+        q, r = np.linalg.qr(rng.standard_normal((3, 3)))
+        q = q * np.sign(np.diag(r))
+        return q if np.linalg.det(q) > 0 else -q
+    s_sets = {
+        "pair_gap_1e-5": [1.2, 1.2 * (1 + 1e-5), 0.9],       # just above the 1e-6 FP64-fallback gap
+        "pair_gap_1e-3": [1.1, 1.1 * (1 + 1e-3), 1.1 * (1 - 1e-3)],
+        "near_iso_1e-4": [1.05, 1.05 * (1 + 1e-4), 1.05 * (1 - 2e-4)],
+        "exact_pair": [1.2, 1.2, 0.9],                         # below the gap: FP64 recompute
+        "isotropic": [1.07, 1.07, 1.07],
+        "rotation": [1.0, 1.0, 1.0],
+        "large_stretch": [2.0, 0.5, 1.0],
+        "compressed": [0.6, 0.7, 0.8],
+    }
+    out = {}
+    for k, s in s_sets.items():
+        F = np.stack([rot() @ np.diag(s) @ rot().T for _ in range(64)])
+        Fg = np.broadcast_to(np.eye(3) * rng.uniform(0.9, 1.1), F.shape).copy()
+        out[k] = (F, Fg)
+    F = np.eye(3) + 0.2 * rng.standard_normal((64, 3, 3))
+    F[np.linalg.det(F) < 0.3] = np.eye(3)
+    out["random"] = (F, np.broadcast_to(np.eye(3), F.shape).copy())
+    return out
+
+
+@pytest.mark.parametrize("case", ["pair_gap_1e-5", "pair_gap_1e-3", "near_iso_1e-4", "exact_pair", "isotropic",
+                                  "rotation", "large_stretch", "compressed", "random"])
+def test_hencky_fp32_spectra_vs_fp64(case):
+    """FP32 Hencky stress and VJP (closed-form eigensolve, FP64 recompute below
+    the singular-value gap threshold) against the FP64 path (Jacobi sweeps),
+    for spectra with close, equal and far-apart singular values."""
+    rng = np.random.default_rng(11)
+    F, Fg = _spectra_cases(rng)[case]
+    C = np.zeros_like(F)
+    tb = rng.standard_normal(F.shape)
+    m = _models()["hencky"]
+    dev = lambda a, dt: torch.tensor(a, dtype=dt, device="cuda")
+    t64 = m.stress(dev(F, torch.float64), dev(Fg, torch.float64), dev(C, torch.float64))
+    b64 = m.stress_vjp(dev(F, torch.float64), dev(Fg, torch.float64), dev(C, torch.float64), dev(tb, torch.float64))
+    # the FP32 path sees the FP32-rounded inputs; compare against FP64 on the same values
+    F32, Fg32, tb32 = (a.astype(np.float32) for a in (F, Fg, tb))
+    t64r = m.stress(dev(F32, torch.float64), dev(Fg32, torch.float64), dev(C, torch.float64))
+    b64r = m.stress_vjp(dev(F32, torch.float64), dev(Fg32, torch.float64), dev(C, torch.float64),
+                        dev(tb32, torch.float64))
+    t32 = m.stress(dev(F32, torch.float32), dev(Fg32, torch.float32), dev(C, torch.float32))
+    b32 = m.stress_vjp(dev(F32, torch.float32), dev(Fg32, torch.float32), dev(C, torch.float32),
+                       dev(tb32, torch.float32))
+    assert torch.isfinite(t32).all() and torch.isfinite(b32[0]).all() and torch.isfinite(b32[1]).all()
+    # error relative to the largest entry of the batch (tau vanishes for a pure rotation)
+    scale = lambda a: max(float(a.abs().max()), 1.0)
+    e_tau = float((t32.double() - t64r).abs().max()) / scale(t64r)
+    e_fb = float((b32[0].double() - b64r[0]).abs().max()) / scale(b64r[0])
+    e_fgb = float((b32[1].double() - b64r[1]).abs().max()) / scale(b64r[1])
+    assert e_tau < 2e-5 and e_fb < 5e-5 and e_fgb < 5e-5, (case, e_tau, e_fb, e_fgb)
+    assert float((t64r - t64).abs().max()) / scale(t64) < 1e-5          # input rounding only
+    assert b64[0].shape == b32[0].shape
+
+
 def test_bin_keys_bit_exact():
     """Cell keys of the device binning equal the oracle's (transfer.py:19-21),
     including particles exactly on half-cell boundaries and outside the grid."""

@@ -268,15 +268,19 @@ int run_radix(MpmPlan* P, const unsigned* kin, const unsigned* vin, unsigned* ko
     const int tile = SORT_THREADS * ITEMS;
     const unsigned* ksrc = kin;
     const unsigned* vsrc = vin;
+    // the movers' sort (a device-side count, typically a few hundred of the nblk
+    // possible 256-key tiles): 4 blocks per SM stride over the active tiles
+    // instead of one block per possible tile
+    const int grid = ITEMS == 1 ? std::max(1, std::min(nblk, P->n_sm * 4)) : nblk;
     for (int pass = 0; pass < P->passes; ++pass) {
         const int shift = pass * RADIX_BITS;
         const bool last = pass == P->passes - 1;
         unsigned* kdst = last ? kout : ((pass & 1) ? a1k : a0k);
         unsigned* vdst = last ? vout : ((pass & 1) ? a1v : a0v);
-        radix_hist_kernel<ITEMS><<<nblk, SORT_THREADS, 0, st>>>(ksrc, P->n, shift, hist, nblk, n_dev);
+        radix_hist_kernel<ITEMS><<<grid, SORT_THREADS, 0, st>>>(ksrc, P->n, shift, hist, nblk, n_dev);
         radix_rowsum_kernel<<<RADIX, 256, 0, st>>>(hist, nblk, totals, tile, n_dev);
         radix_rowscan_kernel<<<RADIX, 256, 0, st>>>(hist, nblk, totals, tile, n_dev);
-        radix_scatter_kernel<ITEMS><<<nblk, SORT_THREADS, 0, st>>>(ksrc, vsrc, P->n, shift, hist, nblk, kdst, vdst,
+        radix_scatter_kernel<ITEMS><<<grid, SORT_THREADS, 0, st>>>(ksrc, vsrc, P->n, shift, hist, nblk, kdst, vdst,
                                                                   n_dev);
         ksrc = kdst;
         vsrc = vdst;

@@ -23,26 +23,31 @@ __device__ __forceinline__ int active_blocks(int nblk, int tile, const int* __re
     return (int)(a < nblk ? a : nblk);
 }
 
-// Per-block digit histogram.  hist is digit-major: hist[d * nblk + b].
-// ITEMS keys per thread; n_dev (may be null): sort the first *n_dev keys.
+// Per-tile digit histogram.  hist is digit-major: hist[d * nblk + b] for tile
+// b of TILE = 256 * ITEMS keys.  n_dev (may be null): sort the first *n_dev
+// keys.  Blocks stride over the active tiles, so a grid smaller than nblk
+// serves a device-side count without launching a block per possible tile.
 template <int ITEMS>
 __global__ void __launch_bounds__(SORT_THREADS)
 radix_hist_kernel(const unsigned* __restrict__ keys, long long n, int shift, unsigned* __restrict__ hist, int nblk,
                   const int* __restrict__ n_dev) {
     constexpr int TILE = SORT_THREADS * ITEMS;
     if (n_dev) n = *n_dev;
-    if ((long long)blockIdx.x * TILE >= n) return;      // past a device-side count
+    const long long tiles = (n + TILE - 1) / TILE;      // active tiles (a device-side count may leave some idle)
     __shared__ unsigned cnt[RADIX];
-    for (int d = threadIdx.x; d < RADIX; d += SORT_THREADS) cnt[d] = 0;
-    __syncthreads();
-    long long base = (long long)blockIdx.x * TILE;
+    for (long long b = blockIdx.x; b < tiles; b += gridDim.x) {
+        for (int d = threadIdx.x; d < RADIX; d += SORT_THREADS) cnt[d] = 0;
+        __syncthreads();
+        const long long base = b * TILE;
 #pragma unroll 4
-    for (int r = 0; r < ITEMS; ++r) {
-        long long q = base + (long long)r * SORT_THREADS + threadIdx.x;
-        if (q < n) atomicAdd(&cnt[(keys[q] >> shift) & (RADIX - 1)], 1u);
+        for (int r = 0; r < ITEMS; ++r) {
+            const long long q = base + (long long)r * SORT_THREADS + threadIdx.x;
+            if (q < n) atomicAdd(&cnt[(keys[q] >> shift) & (RADIX - 1)], 1u);
+        }
+        __syncthreads();
+        for (int d = threadIdx.x; d < RADIX; d += SORT_THREADS) hist[(long long)d * nblk + b] = cnt[d];
+        __syncthreads();
     }
-    __syncthreads();
-    for (int d = threadIdx.x; d < RADIX; d += SORT_THREADS) hist[(long long)d * nblk + blockIdx.x] = cnt[d];
 }
 
 // totals[d] = sum_b hist[d][b]   (one block per digit, fixed-order tree)
@@ -117,66 +122,69 @@ radix_scatter_kernel(const unsigned* __restrict__ keys_in, const unsigned* __res
                      unsigned* __restrict__ keys_out, unsigned* __restrict__ vals_out, const int* __restrict__ n_dev) {
     constexpr int TILE = SORT_THREADS * ITEMS;
     if (n_dev) n = *n_dev;
-    if ((long long)blockIdx.x * TILE >= n) return;
+    const long long tiles = (n + TILE - 1) / TILE;
     constexpr int NW = SORT_THREADS / 32;
     constexpr int PER_WARP = TILE / NW;   // ITEMS rounds of 32 keys
     __shared__ unsigned wcnt[NW][RADIX];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const unsigned lt_mask = (1u << lane) - 1u;
-    for (int i = threadIdx.x; i < NW * RADIX; i += SORT_THREADS) (&wcnt[0][0])[i] = 0;
-    __syncthreads();
-    const long long wbase = (long long)blockIdx.x * TILE + (long long)warp * PER_WARP;
-    unsigned key[ITEMS], val[ITEMS];
-    // pass 1: digit counts of this warp's chunk
+    for (long long b = blockIdx.x; b < tiles; b += gridDim.x) {
+        for (int i = threadIdx.x; i < NW * RADIX; i += SORT_THREADS) (&wcnt[0][0])[i] = 0;
+        __syncthreads();
+        const long long wbase = b * TILE + (long long)warp * PER_WARP;
+        unsigned key[ITEMS], val[ITEMS];
+        // pass 1: digit counts of this warp's chunk
 #pragma unroll
-    for (int r = 0; r < ITEMS; ++r) {
-        const long long q = wbase + (long long)r * 32 + lane;
-        const bool valid = q < n;
-        key[r] = valid ? keys_in[q] : 0u;
-        val[r] = valid ? (vals_in ? vals_in[q] : (unsigned)q) : 0u;
-        const unsigned dig = (key[r] >> shift) & (RADIX - 1);
-        const unsigned vmask = __ballot_sync(0xffffffffu, valid);
-        if (valid) {
-            const unsigned peers = __match_any_sync(vmask, dig);
-            if ((peers & lt_mask) == 0) wcnt[warp][dig] += __popc(peers);
+        for (int r = 0; r < ITEMS; ++r) {
+            const long long q = wbase + (long long)r * 32 + lane;
+            const bool valid = q < n;
+            key[r] = valid ? keys_in[q] : 0u;
+            val[r] = valid ? (vals_in ? vals_in[q] : (unsigned)q) : 0u;
+            const unsigned dig = (key[r] >> shift) & (RADIX - 1);
+            const unsigned vmask = __ballot_sync(0xffffffffu, valid);
+            if (valid) {
+                const unsigned peers = __match_any_sync(vmask, dig);
+                if ((peers & lt_mask) == 0) wcnt[warp][dig] += __popc(peers);
+            }
+            __syncwarp();
         }
-        __syncwarp();
-    }
-    __syncthreads();
-    // per digit: exclusive prefix over the warps, from the block's offset
-    for (int d = threadIdx.x; d < RADIX; d += SORT_THREADS) {
-        unsigned run = offs[(long long)d * nblk + blockIdx.x];
+        __syncthreads();
+        // per digit: exclusive prefix over the warps, from the block's offset
+        for (int d = threadIdx.x; d < RADIX; d += SORT_THREADS) {
+            unsigned run = offs[(long long)d * nblk + b];
 #pragma unroll
-        for (int w = 0; w < NW; ++w) {
-            const unsigned c = wcnt[w][d];
-            wcnt[w][d] = run;
-            run += c;
+            for (int w = 0; w < NW; ++w) {
+                const unsigned c = wcnt[w][d];
+                wcnt[w][d] = run;
+                run += c;
+            }
         }
-    }
-    __syncthreads();
-    // pass 2: scatter
+        __syncthreads();
+        // pass 2: scatter
 #pragma unroll
-    for (int r = 0; r < ITEMS; ++r) {
-        const long long q = wbase + (long long)r * 32 + lane;
-        const bool valid = q < n;
-        const unsigned dig = (key[r] >> shift) & (RADIX - 1);
-        const unsigned vmask = __ballot_sync(0xffffffffu, valid);
-        unsigned peers = 0, rank = 0, base = 0;
-        int leader = lane;
-        if (valid) {
-            peers = __match_any_sync(vmask, dig);
-            rank = __popc(peers & lt_mask);
-            leader = __ffs(peers) - 1;
-            if (rank == 0) base = wcnt[warp][dig];
+        for (int r = 0; r < ITEMS; ++r) {
+            const long long q = wbase + (long long)r * 32 + lane;
+            const bool valid = q < n;
+            const unsigned dig = (key[r] >> shift) & (RADIX - 1);
+            const unsigned vmask = __ballot_sync(0xffffffffu, valid);
+            unsigned peers = 0, rank = 0, base = 0;
+            int leader = lane;
+            if (valid) {
+                peers = __match_any_sync(vmask, dig);
+                rank = __popc(peers & lt_mask);
+                leader = __ffs(peers) - 1;
+                if (rank == 0) base = wcnt[warp][dig];
+            }
+            base = __shfl_sync(0xffffffffu, base, leader);
+            if (valid && MPM_INB((long long)base + rank, n, 10)) {
+                keys_out[base + rank] = key[r];
+                vals_out[base + rank] = val[r];
+            }
+            __syncwarp();
+            if (valid && rank == 0) wcnt[warp][dig] = base + __popc(peers);
+            __syncwarp();
         }
-        base = __shfl_sync(0xffffffffu, base, leader);
-        if (valid && MPM_INB((long long)base + rank, n, 10)) {
-            keys_out[base + rank] = key[r];
-            vals_out[base + rank] = val[r];
-        }
-        __syncwarp();
-        if (valid && rank == 0) wcnt[warp][dig] = base + __popc(peers);
-        __syncwarp();
+        __syncthreads();
     }
 }
 

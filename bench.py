@@ -256,7 +256,7 @@ def kernel_bytes_per_particle(kind, w):
 # traffic grows in proportion to the particles, so it is scaled to the workload.
 MEASURED_TRAFFIC_PER_PARTICLE = {
     # the neo-Hookean and the Hencky run of one reverse step (the kernel specialised per model)
-    "bwd_particle": (281422336 + 91672832 + 244270848 + 82131456) / 2092825,
+    "bwd_particle": (281440768 + 89405440 + 244199680 + 81494016) / 2092825,
     "g2p": (137.490688e6 + 339.093504e6) / 2092825,
 }
 

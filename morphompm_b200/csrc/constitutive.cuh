@@ -371,6 +371,54 @@ struct Hencky {
     }
 };
 
+// FP64 recompute of an FP32 Hencky particle (stress, VJP): float in and out,
+// double inside.  The stable divided difference is used here too (the
+// recompute of a near-degenerate particle must not fall back to the 1e-9
+// switch).
+__device__ __forceinline__ void hencky_stress_fp64(const float F[9], const float Fg[9], float mu, float lam,
+                                                   float tau[9]) {
+    double Fd[9], Fgd[9], Fgid[9], Fed[9], bd[3], Vd[9], td[9];
+#pragma unroll
+    for (int i = 0; i < 9; ++i) { Fd[i] = F[i]; Fgd[i] = Fg[i]; }
+    hencky_eig(Fd, Fgd, Fgid, Fed, bd, Vd);
+    hencky_tau_from_eig(bd, Vd, (double)mu, (double)lam, td);
+#pragma unroll
+    for (int i = 0; i < 9; ++i) tau[i] = (float)td[i];
+}
+__device__ __forceinline__ void hencky_vjp_fp64(const float F[9], const float Fg[9], float mu, float lam,
+                                                const float tb[9], float Fb[9], float Fgb[9]) {
+    double Fd[9], Fgd[9], Fgid[9], Fed[9], bd[3], Vd[9], tbd[9], Fbd[9], Fgbd[9];
+#pragma unroll
+    for (int i = 0; i < 9; ++i) { Fd[i] = F[i]; Fgd[i] = Fg[i]; tbd[i] = tb[i]; }
+    hencky_eig(Fd, Fgd, Fgid, Fed, bd, Vd);
+    double tbs[9];
+    sym(tbd, tbs);
+    double tr = tbs[0] + tbs[4] + tbs[8];
+    double M[9];
+#pragma unroll
+    for (int i = 0; i < 9; ++i) M[i] = (double)mu * tbs[i] + ((i % 4 == 0) ? 0.5 * (double)lam * tr : 0.0);
+    double T[9], UtMU[9];
+    mTm(Vd, M, T);
+    mm(T, Vd, UtMU);
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            double bi = bd[i], bj = bd[j];
+            double L = (bi == bj) ? 1.0 / bi : log1p((bi - bj) / bj) / (bj * ((bi - bj) / bj));
+            UtMU[3 * i + j] *= L;
+        }
+    double Bb[9], Feb[9];
+    mm(Vd, UtMU, T);
+    mmT(T, Vd, Bb);
+    mm(Bb, Fed, Feb);
+#pragma unroll
+    for (int i = 0; i < 9; ++i) Feb[i] *= 2.0;
+    pull_back(Fd, Fgid, Feb, Fbd, Fgbd);
+#pragma unroll
+    for (int i = 0; i < 9; ++i) { Fb[i] = (float)Fbd[i]; Fgb[i] = (float)Fgbd[i]; }
+}
+
 template <>
 struct Hencky<float> {
     static __device__ __forceinline__ bool stress(const float F[9], const float Fg[9], float mu, float lam,
@@ -381,13 +429,7 @@ struct Hencky<float> {
             hencky_tau_from_eig(beta, V, mu, lam, tau);
             return false;
         }
-        double Fd[9], Fgd[9], Fgid[9], Fed[9], bd[3], Vd[9], td[9];
-#pragma unroll
-        for (int i = 0; i < 9; ++i) { Fd[i] = F[i]; Fgd[i] = Fg[i]; }
-        hencky_eig(Fd, Fgd, Fgid, Fed, bd, Vd);
-        hencky_tau_from_eig(bd, Vd, (double)mu, (double)lam, td);
-#pragma unroll
-        for (int i = 0; i < 9; ++i) tau[i] = (float)td[i];
+        hencky_stress_fp64(F, Fg, mu, lam, tau);
         return true;
     }
     static __device__ __forceinline__ bool vjp(const float F[9], const float Fg[9], float mu, float lam,
@@ -398,38 +440,7 @@ struct Hencky<float> {
             hencky_vjp_from_eig(F, Fgi, Fe, beta, V, mu, lam, tb, Fb, Fgb);
             return false;
         }
-        double Fd[9], Fgd[9], Fgid[9], Fed[9], bd[3], Vd[9], tbd[9], Fbd[9], Fgbd[9];
-#pragma unroll
-        for (int i = 0; i < 9; ++i) { Fd[i] = F[i]; Fgd[i] = Fg[i]; tbd[i] = tb[i]; }
-        hencky_eig(Fd, Fgd, Fgid, Fed, bd, Vd);
-        // the stable divided difference is used here too (the FP64 recompute of
-        // a near-degenerate particle must not fall back to the 1e-9 switch)
-        double tbs[9];
-        sym(tbd, tbs);
-        double tr = tbs[0] + tbs[4] + tbs[8];
-        double M[9];
-#pragma unroll
-        for (int i = 0; i < 9; ++i) M[i] = (double)mu * tbs[i] + ((i % 4 == 0) ? 0.5 * (double)lam * tr : 0.0);
-        double T[9], UtMU[9];
-        mTm(Vd, M, T);
-        mm(T, Vd, UtMU);
-#pragma unroll
-        for (int i = 0; i < 3; ++i)
-#pragma unroll
-            for (int j = 0; j < 3; ++j) {
-                double bi = bd[i], bj = bd[j];
-                double L = (bi == bj) ? 1.0 / bi : log1p((bi - bj) / bj) / (bj * ((bi - bj) / bj));
-                UtMU[3 * i + j] *= L;
-            }
-        double Bb[9], Feb[9];
-        mm(Vd, UtMU, T);
-        mmT(T, Vd, Bb);
-        mm(Bb, Fed, Feb);
-#pragma unroll
-        for (int i = 0; i < 9; ++i) Feb[i] *= 2.0;
-        pull_back(Fd, Fgid, Feb, Fbd, Fgbd);
-#pragma unroll
-        for (int i = 0; i < 9; ++i) { Fb[i] = (float)Fbd[i]; Fgb[i] = (float)Fgbd[i]; }
+        hencky_vjp_fp64(F, Fg, mu, lam, tb, Fb, Fgb);
         return true;
     }
 };
@@ -512,7 +523,8 @@ __device__ __forceinline__ bool hencky_stress_keep(const R* F, const R* Fg, R mu
     bool fp64 = false;
     if constexpr (sizeof(R) == 4) fp64 = sv_gap(beta) < thresh;
     if (fp64) {
-        Hencky<R>::stress(F, Fg, mu, lam, thresh, tau);
+        // the FP32 solve above already failed the gap test: straight to FP64
+        if constexpr (sizeof(R) == 4) hencky_stress_fp64(F, Fg, mu, lam, tau);
     } else {
         hencky_tau_from_eig(beta, V, mu, lam, tau);
     }
@@ -526,7 +538,12 @@ __device__ __forceinline__ bool hencky_stress_keep(const R* F, const R* Fg, R mu
 template <typename R>
 __device__ __forceinline__ bool hencky_vjp_keep(const R* F, const R* Fg, R mu, R lam, float thresh, const R* tb,
                                              const R* keep, R* Fb, R* Fgb) {
-    if (keep[12] != R(0)) return Hencky<R>::vjp(F, Fg, mu, lam, thresh, tb, Fb, Fgb);
+    if constexpr (sizeof(R) == 4) {
+        if (keep[12] != R(0)) {         // the stress went to FP64: so does the VJP
+            hencky_vjp_fp64(F, Fg, mu, lam, tb, Fb, Fgb);
+            return true;
+        }
+    }
     R Fgi[9], Fe[9], beta[3], V[9];
     inv3(Fg, Fgi);
     mm(F, Fgi, Fe);

@@ -357,7 +357,8 @@ int run_resort(MpmPlan* P, const char* old_tape, char* tape, const unsigned* key
     const unsigned char* sflag = at<const unsigned char>(P, P->o_mflag);
     const unsigned char* pflag = at<const unsigned char>(P, P->o_pflag);
     int* status = at<int>(P, P->o_status);
-    Site site(P, MPM_K_SORT, 7 + 4 * P->passes, st);
+    // count, two scans, compact; per radix pass hist, row sums, row scans, scatter; the two placements
+    Site site(P, MPM_K_SORT, 6 + 4 * P->passes, st);
     const int nb = P->nblk_resort;
     resort_count_kernel<<<nb, RESORT_THREADS, 0, st>>>(sflag, pflag, P->n, mask, pmask, rblk, pblk);
     scan_counts_kernel<<<1, 1024, 0, st>>>(rblk, nb, n_movers + 1, INT_MAX, status);

@@ -291,8 +291,16 @@ __device__ __forceinline__ float dk_entry<float>(float bi, float bj, float, floa
     float d = (bi - bj) / bj;
     return log1pf(d) / (bj * d);
 }
+// the cancellation-free form in FP64 (the FP64 recompute of an FP32 particle
+// near degeneracy must not fall back to the 1e-9 switch)
+__device__ __forceinline__ double dk_stable(double bi, double bj) {
+    if (bi == bj) return 1.0 / bi;
+    const double d = (bi - bj) / bj;
+    return log1p(d) / (bj * d);
+}
 
-template <typename R>
+// STABLE: the cancellation-free divided difference also in FP64.
+template <typename R, bool STABLE = false>
 __device__ __forceinline__ void hencky_vjp_from_eig(const R F[9], const R Fgi[9], const R Fe[9], const R beta[3],
                                                     const R V[9], R mu, R lam, const R tau_bar[9],
                                                     R Fb[9], R Fgb[9]) {
@@ -312,13 +320,21 @@ __device__ __forceinline__ void hencky_vjp_from_eig(const R F[9], const R Fgi[9]
             UtMU[3 * i + j] = T[3 * i] * V[j] + T[3 * i + 1] * V[3 + j] + T[3 * i + 2] * V[6 + j];
             UtMU[3 * j + i] = UtMU[3 * i + j];
         }
-    R lb[3] = {d_log(beta[0]), d_log(beta[1]), d_log(beta[2])};
+    R lb[3];
+    if constexpr (!STABLE) {
+#pragma unroll
+        for (int i = 0; i < 3; ++i) lb[i] = d_log(beta[i]);
+    }
+    auto dk = [&](int i, int j) -> R {
+        if constexpr (STABLE) return dk_stable(beta[i], beta[j]);
+        else return dk_entry<R>(beta[i], beta[j], lb[i], lb[j]);
+    };
 #pragma unroll
     for (int i = 0; i < 3; ++i) {
-        UtMU[4 * i] *= dk_entry<R>(beta[i], beta[i], lb[i], lb[i]);
+        UtMU[4 * i] *= dk(i, i);
 #pragma unroll
         for (int j = i + 1; j < 3; ++j) {
-            const R L = dk_entry<R>(beta[i], beta[j], lb[i], lb[j]);
+            const R L = dk(i, j);
             UtMU[3 * i + j] *= L;
             UtMU[3 * j + i] *= L;
         }
@@ -391,30 +407,7 @@ __device__ __forceinline__ void hencky_vjp_fp64(const float F[9], const float Fg
 #pragma unroll
     for (int i = 0; i < 9; ++i) { Fd[i] = F[i]; Fgd[i] = Fg[i]; tbd[i] = tb[i]; }
     hencky_eig(Fd, Fgd, Fgid, Fed, bd, Vd);
-    double tbs[9];
-    sym(tbd, tbs);
-    double tr = tbs[0] + tbs[4] + tbs[8];
-    double M[9];
-#pragma unroll
-    for (int i = 0; i < 9; ++i) M[i] = (double)mu * tbs[i] + ((i % 4 == 0) ? 0.5 * (double)lam * tr : 0.0);
-    double T[9], UtMU[9];
-    mTm(Vd, M, T);
-    mm(T, Vd, UtMU);
-#pragma unroll
-    for (int i = 0; i < 3; ++i)
-#pragma unroll
-        for (int j = 0; j < 3; ++j) {
-            double bi = bd[i], bj = bd[j];
-            double L = (bi == bj) ? 1.0 / bi : log1p((bi - bj) / bj) / (bj * ((bi - bj) / bj));
-            UtMU[3 * i + j] *= L;
-        }
-    double Bb[9], Feb[9];
-    mm(Vd, UtMU, T);
-    mmT(T, Vd, Bb);
-    mm(Bb, Fed, Feb);
-#pragma unroll
-    for (int i = 0; i < 9; ++i) Feb[i] *= 2.0;
-    pull_back(Fd, Fgid, Feb, Fbd, Fgbd);
+    hencky_vjp_from_eig<double, true>(Fd, Fgid, Fed, bd, Vd, (double)mu, (double)lam, tbd, Fbd, Fgbd);
 #pragma unroll
     for (int i = 0; i < 9; ++i) { Fb[i] = (float)Fbd[i]; Fgb[i] = (float)Fgbd[i]; }
 }
@@ -492,18 +485,15 @@ __device__ __forceinline__ void hb_vjp(const R F[9], const R Fg[9], const R C[9]
 }
 
 // ---------------------------------------------------------------------------
-// Out-of-line Hencky evaluations.  An out-of-line call passes its arrays
-// through the local-memory stack, so the FP32 eigensolves stay inline; the
-// stand-alone Hencky VJP and the rare FP64 recompute of the stress in the
-// forward kernels go through these so that their register demand does not
-// inflate the allocation of the kernels that fuse them.  (The reverse kernel's
-// kept-eigensystem pair below inlines its FP64 branch: out of line it has no
-// spills but runs 4% slower.)
+// Out-of-line Hencky VJP for the run-time model switch (the stand-alone VJP
+// and the kernels over mixed or external scenes), so that its register demand
+// does not inflate the allocation of the kernels that fuse it.  The FP64
+// recompute of the stress is inline in every kernel, and so is the VJP's in
+// the model-specialised reverse kernels: out of line, such a call passes its
+// arrays through the local-memory stack and measured slower even on the rare
+// path (reverse kernel 179.3 -> 186.2 ms, G2P 93.6 -> 96.7 ms per config-4
+// trajectory).
 // ---------------------------------------------------------------------------
-template <typename R>
-__device__ __noinline__ bool hencky_stress_ool(const R* F, const R* Fg, R mu, R lam, float thresh, R* tau) {
-    return Hencky<R>::stress(F, Fg, mu, lam, thresh, tau);
-}
 template <typename R>
 __device__ __noinline__ bool hencky_vjp_ool(const R* F, const R* Fg, R mu, R lam, float thresh, const R* tb, R* Fb,
                                             R* Fgb) {
@@ -568,7 +558,10 @@ __device__ __forceinline__ bool model_stress(const ModelParams<R>& P, float thre
         R Fgi[9], Fe[9], beta[3], V[9];
         hencky_eig(F, Fg, Fgi, Fe, beta, V);
         if constexpr (sizeof(R) == 4) {
-            if (sv_gap(beta) < thresh) return hencky_stress_ool<R>(F, Fg, P.mu, P.lam, thresh, tau);
+            if (sv_gap(beta) < thresh) {     // rare: straight to FP64, inline
+                hencky_stress_fp64(F, Fg, P.mu, P.lam, tau);
+                return true;
+            }
         }
         hencky_tau_from_eig(beta, V, P.mu, P.lam, tau);
         return false;

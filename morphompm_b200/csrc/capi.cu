@@ -631,7 +631,7 @@ int mpm_plan_create(const MpmScene* scenes, int32_t n_scenes, int32_t real_bytes
     P->o_scene_of = L.take(n * 4);
     P->o_tile_scene = L.take(nt * 4);
     P->o_status = L.take(128);
-    P->nblk_seg = (int)((P->n + SEG_TILE - 1) / SEG_TILE);
+    P->nblk_seg = (int)((P->n + SEGK_TILE - 1) / SEGK_TILE);
     P->o_cell_seg = L.take((size_t)P->n_keys * 4);
     P->o_blk = L.take((size_t)P->nblk_seg * 4);
     P->nblk_tile = (int)((P->n_tiles + SEG_TILE - 1) / SEG_TILE);
@@ -1276,7 +1276,7 @@ bool noalloc_layout(MpmPlan& P, const MpmScene& sc, int real_bytes, SceneAux& a)
     P.key_bits = bits;
     P.passes = (bits + RADIX_BITS - 1) / RADIX_BITS;
     P.nblk_sort = (int)((P.n + SORT_TILE - 1) / SORT_TILE);
-    P.nblk_seg = (int)((P.n + SEG_TILE - 1) / SEG_TILE);
+    P.nblk_seg = (int)((P.n + SEGK_TILE - 1) / SEGK_TILE);
     P.active_cap = (int)P.n_tiles;
     const size_t R = (size_t)real_bytes, n = (size_t)P.n, nt = (size_t)P.n_tiles;
     Layout tl;

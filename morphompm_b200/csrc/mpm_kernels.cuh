@@ -195,28 +195,62 @@ constexpr int SEG_THREADS = 256;
 constexpr int SEG_ITEMS = 16;
 constexpr int SEG_TILE = SEG_THREADS * SEG_ITEMS;
 
-// is slot s the start of an inside segment?
-__device__ __forceinline__ bool seg_start(const Ctx& ctx, const unsigned* __restrict__ skeys, long long s,
-                                          unsigned k) {
-    if (s > 0 && skeys[s - 1] == k) return false;
-    const SceneAux& ax = ctx.aux[ctx.scene_of[s]];
-    return (long long)k - ax.cell_begin < ax.ncells;
+// Segment kernels: SEGK_ITEMS warp-striped rounds of slots per block (slot =
+// block base + round*256 + thread, every key load coalesced), all their loads
+// issued before any is used, few registers: a block waits on one chain of
+// memory latencies (key, then its scene), not one per round.
+#ifndef MPM_SEGK_ITEMS
+#define MPM_SEGK_ITEMS 4
+#endif
+constexpr int SEGK_ITEMS = MPM_SEGK_ITEMS;
+constexpr int SEGK_TILE = SEG_THREADS * SEGK_ITEMS;
+
+// Bit r of start / last: slot base + r*256 + thread starts / ends an inside
+// segment (a run of equal keys whose cell lies in its scene's grid).
+__device__ __forceinline__ void seg_flags(const Ctx& ctx, const unsigned* __restrict__ skeys, long long base,
+                                          unsigned key[SEGK_ITEMS], unsigned& start, unsigned& last) {
+    const int lane = threadIdx.x & 31;
+    const long long n = ctx.n;
+    unsigned edge[SEGK_ITEMS];
+    int sid[SEGK_ITEMS];
+#pragma unroll
+    for (int r = 0; r < SEGK_ITEMS; ++r) {
+        const long long s = base + (long long)r * SEG_THREADS + threadIdx.x;
+        const bool valid = s < n;
+        key[r] = valid ? skeys[s] : 0u;
+        sid[r] = valid ? ctx.scene_of[s] : 0;
+        // lane 0 needs the key before it, lane 31 the key after it
+        const long long e = lane == 0 ? s - 1 : s + 1;
+        edge[r] = ((lane == 0 || lane == 31) && e >= 0 && e < n) ? skeys[e] : 0u;
+    }
+    start = 0;
+    last = 0;
+#pragma unroll
+    for (int r = 0; r < SEGK_ITEMS; ++r) {
+        const long long s = base + (long long)r * SEG_THREADS + threadIdx.x;
+        unsigned prv = __shfl_up_sync(0xffffffffu, key[r], 1);
+        unsigned nxt = __shfl_down_sync(0xffffffffu, key[r], 1);
+        if (lane == 0) prv = edge[r];
+        if (lane == 31) nxt = edge[r];
+        const bool valid = s < n;
+        const bool a = valid && (s == 0 || prv != key[r]);
+        const bool b = valid && (s == n - 1 || nxt != key[r]);
+        if (a || b) {
+            const SceneAux& ax = ctx.aux[sid[r]];
+            if ((long long)key[r] - ax.cell_begin < ax.ncells) {
+                start |= (a ? 1u : 0u) << r;
+                last |= (b ? 1u : 0u) << r;
+            }
+        }
+    }
 }
 
-// Slots of a block are visited warp-striped (slot = block base + round*256 +
-// thread), so every load of the sorted keys is coalesced.
 __global__ void __launch_bounds__(SEG_THREADS)
 seg_count_kernel(Ctx ctx, const unsigned* __restrict__ skeys) {
     __shared__ unsigned red[SEG_THREADS / 32];
-    const long long base = (long long)blockIdx.x * SEG_TILE;
-    unsigned cnt = 0;
-#pragma unroll 4
-    for (int r = 0; r < SEG_ITEMS; ++r) {
-        long long s = base + (long long)r * SEG_THREADS + threadIdx.x;
-        if (s >= ctx.n) break;
-        unsigned k = skeys[s];
-        if (seg_start(ctx, skeys, s, k)) ++cnt;
-    }
+    unsigned key[SEGK_ITEMS], start, last;
+    seg_flags(ctx, skeys, (long long)blockIdx.x * SEGK_TILE, key, start, last);
+    unsigned cnt = __popc(start);
     for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
     if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = cnt;
     __syncthreads();
@@ -375,47 +409,51 @@ tile_write_kernel(int* __restrict__ flag, long long n_tiles, const unsigned* __r
     }
 }
 
+// Writes seg_first / seg_last / cell_seg.  A slot's segment id is the number of
+// segment starts up to and including it: the block's count from the scan, the
+// starts of the earlier (round, warp) pairs of the block (one exclusive scan
+// of the SEGK_ITEMS x 8 warp counts, one per lane of warp 0) and the lanes
+// before it.
 __global__ void __launch_bounds__(SEG_THREADS)
 seg_write_kernel(Ctx ctx, const unsigned* __restrict__ skeys) {
     constexpr int NW = SEG_THREADS / 32;
-    __shared__ unsigned wtot[NW];
+    constexpr int E = SEGK_ITEMS * NW;
+    static_assert(E <= 32, "one (round, warp) count per lane of the scanning warp");
+    __shared__ unsigned pre[SEGK_ITEMS * NW];      // round-major
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const unsigned lt = (1u << lane) - 1u;
-    const long long base = (long long)blockIdx.x * SEG_TILE;
-    unsigned run = ctx.blk_count[blockIdx.x];     // segments started before this round
-    for (int r = 0; r < SEG_ITEMS; ++r) {
-        const long long s = base + (long long)r * SEG_THREADS + threadIdx.x;
-        const bool valid = s < ctx.n;
-        const unsigned k = valid ? skeys[s] : 0u;
-        const bool start = valid && seg_start(ctx, skeys, s, k);
-        const unsigned ball = __ballot_sync(0xffffffffu, start);
-        if (lane == 0) wtot[warp] = __popc(ball);
-        __syncthreads();
-        unsigned before = run;
-        unsigned round = 0;
+    const long long base = (long long)blockIdx.x * SEGK_TILE;
+    unsigned key[SEGK_ITEMS], start, last;
+    seg_flags(ctx, skeys, base, key, start, last);
 #pragma unroll
-        for (int w = 0; w < NW; ++w) {
-            const unsigned c = wtot[w];
-            if (w < warp) before += c;
-            round += c;
+    for (int r = 0; r < SEGK_ITEMS; ++r) {
+        const unsigned ball = __ballot_sync(0xffffffffu, (start >> r) & 1u);
+        if (lane == 0) pre[r * NW + warp] = __popc(ball);
+    }
+    __syncthreads();
+    if (warp == 0) {
+        const unsigned v = lane < E ? pre[lane] : 0u;
+        unsigned inc = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned t = __shfl_up_sync(0xffffffffu, inc, o);
+            if (lane >= o) inc += t;
         }
-        before += __popc(ball & lt);
-        // starts up to and including s, minus one: the segment id of slot s
-        const unsigned id = before + (start ? 1u : 0u);
-        if (start && MPM_INB(id - 1, ctx.n, 3)) {
+        if (lane < E) pre[lane] = inc - v;
+    }
+    __syncthreads();
+    const unsigned run = ctx.blk_count[blockIdx.x];     // segments started before this block
+#pragma unroll
+    for (int r = 0; r < SEGK_ITEMS; ++r) {
+        const long long s = base + (long long)r * SEG_THREADS + threadIdx.x;
+        const bool st = (start >> r) & 1u;
+        const unsigned ball = __ballot_sync(0xffffffffu, st);
+        const unsigned id = run + pre[r * NW + warp] + __popc(ball & lt) + (st ? 1u : 0u);
+        if (st && MPM_INB(id - 1, ctx.n, 3)) {
             ctx.seg_first[id - 1] = (int)s;
-            if (MPM_INB(k, ctx.n_keys, 2)) ctx.cell_seg[k] = (int)id;
+            if (MPM_INB(key[r], ctx.n_keys, 2)) ctx.cell_seg[key[r]] = (int)id;
         }
-        if (valid && id > 0) {
-            const bool last = s == ctx.n - 1 || skeys[s + 1] != k;
-            if (last) {
-                const SceneAux& ax = ctx.aux[ctx.scene_of[s]];
-                if ((long long)k - ax.cell_begin < ax.ncells && MPM_INB(id - 1, ctx.n, 3))
-                    ctx.seg_last[id - 1] = (int)(s + 1);
-            }
-        }
-        run += round;
-        __syncthreads();
+        if (((last >> r) & 1u) && id > 0 && MPM_INB(id - 1, ctx.n, 3)) ctx.seg_last[id - 1] = (int)(s + 1);
     }
 }
 

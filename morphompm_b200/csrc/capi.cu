@@ -634,7 +634,7 @@ int mpm_plan_create(const MpmScene* scenes, int32_t n_scenes, int32_t real_bytes
     P->nblk_seg = (int)((P->n + SEGK_TILE - 1) / SEGK_TILE);
     P->o_cell_seg = L.take((size_t)P->n_keys * 4);
     P->o_blk = L.take((size_t)P->nblk_seg * 4);
-    P->nblk_tile = (int)((P->n_tiles + SEG_TILE - 1) / SEG_TILE);
+    P->nblk_tile = (int)((P->n_tiles + TILEK_TILE - 1) / TILEK_TILE);
     P->o_tblk = L.take((size_t)P->nblk_tile * 4);
     P->o_tile_flag = L.take(nt * 4);
     P->o_keys = L.take(n * 4);
@@ -1297,7 +1297,7 @@ bool noalloc_layout(MpmPlan& P, const MpmScene& sc, int real_bytes, SceneAux& a)
     P.o_status = L.take(128);
     P.o_cell_seg = L.take((size_t)P.n_keys * 4);
     P.o_blk = L.take((size_t)P.nblk_seg * 4);
-    P.nblk_tile = (int)((P.n_tiles + SEG_TILE - 1) / SEG_TILE);
+    P.nblk_tile = (int)((P.n_tiles + TILEK_TILE - 1) / TILEK_TILE);
     P.o_tblk = L.take((size_t)P.nblk_tile * 4);
     P.o_tile_flag = L.take(nt * 4);
     P.o_keys = L.take(n * 4);

@@ -192,8 +192,6 @@ __global__ void bin_keys_single(MpmScene sc, long long n, const R* __restrict__ 
 // entirely off the grid) form no segment.
 // ---------------------------------------------------------------------------
 constexpr int SEG_THREADS = 256;
-constexpr int SEG_ITEMS = 16;
-constexpr int SEG_TILE = SEG_THREADS * SEG_ITEMS;
 
 // Segment kernels: SEGK_ITEMS warp-striped rounds of slots per block (slot =
 // block base + round*256 + thread, every key load coalesced), all their loads
@@ -316,23 +314,43 @@ scan_counts_kernel(unsigned* __restrict__ cnt, int nblk, int* __restrict__ total
 __global__ void __launch_bounds__(256)
 remark_cells_kernel(Ctx ctx, const unsigned* __restrict__ skeys) {
     const int nseg = *ctx.n_seg;
-    for (int id = blockIdx.x * blockDim.x + threadIdx.x; id < nseg; id += gridDim.x * blockDim.x) {
-        const int f = ctx.seg_first[id];
-        if (!MPM_INB(f, ctx.n, 11)) continue;
-        const unsigned k = skeys[f];
-        if (MPM_INB(k, ctx.n_keys, 2)) ctx.cell_seg[k] = id + 1;
+#ifndef MPM_REMARK_BATCH
+#define MPM_REMARK_BATCH 4
+#endif
+    // MPM_REMARK_BATCH segments per thread and pass, their loads issued together
+    constexpr int NB = MPM_REMARK_BATCH;
+    const int stride = gridDim.x * blockDim.x;
+    for (int id0 = blockIdx.x * blockDim.x + threadIdx.x; id0 < nseg; id0 += NB * stride) {
+        int f[NB];
+#pragma unroll
+        for (int b = 0; b < NB; ++b) {
+            const int id = id0 + b * stride;
+            f[b] = id < nseg ? ctx.seg_first[id] : -1;
+        }
+        unsigned k[NB];
+#pragma unroll
+        for (int b = 0; b < NB; ++b) k[b] = (f[b] >= 0 && MPM_INB(f[b], ctx.n, 11)) ? skeys[f[b]] : 0xffffffffu;
+#pragma unroll
+        for (int b = 0; b < NB; ++b)
+            if (f[b] >= 0 && k[b] != 0xffffffffu && MPM_INB(k[b], ctx.n_keys, 2)) ctx.cell_seg[k[b]] = id0 + b * stride + 1;
     }
 }
 
-// exclusive scan, in place, of the block's SEG_ITEMS x 8 (round, warp) counts
-// (round-major, 128 entries, four per lane of warp 0); call from all threads
+// exclusive scan, in place, of a block's E (round, warp) counts (round-major;
+// warp 0, E / 32 per lane, or one per lane for E <= 32); call from all threads
+template <int E>
 __device__ __forceinline__ void scan_round_warp_counts(unsigned* pre) {
+    static_assert(E <= 32 || E % 32 == 0, "E <= 32 or a multiple of 32");
+    constexpr int PER = E <= 32 ? 1 : E / 32;
     __syncthreads();
     const int lane = threadIdx.x & 31;
     if ((threadIdx.x >> 5) == 0) {
-        unsigned v[4], tot = 0;
+        unsigned v[PER], tot = 0;
 #pragma unroll
-        for (int j = 0; j < 4; ++j) { v[j] = pre[4 * lane + j]; tot += v[j]; }
+        for (int j = 0; j < PER; ++j) {
+            v[j] = PER * lane + j < E ? pre[PER * lane + j] : 0u;
+            tot += v[j];
+        }
         unsigned inc = tot;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
@@ -341,34 +359,42 @@ __device__ __forceinline__ void scan_round_warp_counts(unsigned* pre) {
         }
         unsigned ex = inc - tot;
 #pragma unroll
-        for (int j = 0; j < 4; ++j) { pre[4 * lane + j] = ex; ex += v[j]; }
+        for (int j = 0; j < PER; ++j) {
+            if (PER * lane + j < E) pre[PER * lane + j] = ex;
+            ex += v[j];
+        }
     }
     __syncthreads();
 }
 
 // Active-tile list: the flagged tiles, in tile order.  Per-block counts, the
 // block scan above, then ranks from warp ballots; the flags are reset for the
-// next step.  A block covers SEG_ITEMS warp-striped rounds of tiles (every load
-// coalesced), and all its flag loads are issued before any is used; one scan
-// of the (round, warp) counts replaces a barrier pair per round.
+// next step.  A block covers TILEK_ITEMS warp-striped rounds of tiles (every
+// load coalesced), and all its flag loads are issued before any is used; one
+// scan of the (round, warp) counts replaces a barrier pair per round.
+#ifndef MPM_TILEK_ITEMS
+#define MPM_TILEK_ITEMS 4
+#endif
+constexpr int TILEK_ITEMS = MPM_TILEK_ITEMS;
+constexpr int TILEK_TILE = SEG_THREADS * TILEK_ITEMS;
 // Bit r: tile base + r*256 + thread is flagged.
 __device__ __forceinline__ unsigned tile_flags(const int* __restrict__ flag, long long n_tiles, long long base) {
     unsigned on = 0;
-    int f[SEG_ITEMS];
+    int f[TILEK_ITEMS];
 #pragma unroll
-    for (int r = 0; r < SEG_ITEMS; ++r) {
+    for (int r = 0; r < TILEK_ITEMS; ++r) {
         const long long t = base + (long long)r * SEG_THREADS + threadIdx.x;
         f[r] = t < n_tiles ? flag[t] : 0;
     }
 #pragma unroll
-    for (int r = 0; r < SEG_ITEMS; ++r) on |= (f[r] != 0 ? 1u : 0u) << r;
+    for (int r = 0; r < TILEK_ITEMS; ++r) on |= (f[r] != 0 ? 1u : 0u) << r;
     return on;
 }
 
 __global__ void __launch_bounds__(SEG_THREADS)
 tile_count_kernel(const int* __restrict__ flag, long long n_tiles, unsigned* __restrict__ blk) {
     __shared__ unsigned red[SEG_THREADS / 32];
-    unsigned cnt = __popc(tile_flags(flag, n_tiles, (long long)blockIdx.x * SEG_TILE));
+    unsigned cnt = __popc(tile_flags(flag, n_tiles, (long long)blockIdx.x * TILEK_TILE));
     for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
     if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = cnt;
     __syncthreads();
@@ -383,21 +409,20 @@ __global__ void __launch_bounds__(SEG_THREADS)
 tile_write_kernel(int* __restrict__ flag, long long n_tiles, const unsigned* __restrict__ blk,
                   int* __restrict__ active, int cap) {
     constexpr int NW = SEG_THREADS / 32;
-    static_assert(SEG_ITEMS * NW == 128, "four (round, warp) counts per lane of the scanning warp");
-    __shared__ unsigned pre[SEG_ITEMS * NW];
+    __shared__ unsigned pre[TILEK_ITEMS * NW];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const unsigned lt = (1u << lane) - 1u;
-    const long long base = (long long)blockIdx.x * SEG_TILE;
+    const long long base = (long long)blockIdx.x * TILEK_TILE;
     const unsigned on = tile_flags(flag, n_tiles, base);
 #pragma unroll
-    for (int r = 0; r < SEG_ITEMS; ++r) {
+    for (int r = 0; r < TILEK_ITEMS; ++r) {
         const unsigned ball = __ballot_sync(0xffffffffu, (on >> r) & 1u);
         if (lane == 0) pre[r * NW + warp] = __popc(ball);
     }
-    scan_round_warp_counts(pre);
+    scan_round_warp_counts<TILEK_ITEMS * NW>(pre);
     const unsigned run = blk[blockIdx.x];
 #pragma unroll
-    for (int r = 0; r < SEG_ITEMS; ++r) {
+    for (int r = 0; r < TILEK_ITEMS; ++r) {
         const long long t = base + (long long)r * SEG_THREADS + threadIdx.x;
         const bool a = (on >> r) & 1u;
         const unsigned ball = __ballot_sync(0xffffffffu, a);
@@ -412,13 +437,11 @@ tile_write_kernel(int* __restrict__ flag, long long n_tiles, const unsigned* __r
 // Writes seg_first / seg_last / cell_seg.  A slot's segment id is the number of
 // segment starts up to and including it: the block's count from the scan, the
 // starts of the earlier (round, warp) pairs of the block (one exclusive scan
-// of the SEGK_ITEMS x 8 warp counts, one per lane of warp 0) and the lanes
-// before it.
+// of the SEGK_ITEMS x 8 warp counts) and the lanes before it.
 __global__ void __launch_bounds__(SEG_THREADS)
 seg_write_kernel(Ctx ctx, const unsigned* __restrict__ skeys) {
     constexpr int NW = SEG_THREADS / 32;
     constexpr int E = SEGK_ITEMS * NW;
-    static_assert(E <= 32, "one (round, warp) count per lane of the scanning warp");
     __shared__ unsigned pre[SEGK_ITEMS * NW];      // round-major
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const unsigned lt = (1u << lane) - 1u;
@@ -430,18 +453,7 @@ seg_write_kernel(Ctx ctx, const unsigned* __restrict__ skeys) {
         const unsigned ball = __ballot_sync(0xffffffffu, (start >> r) & 1u);
         if (lane == 0) pre[r * NW + warp] = __popc(ball);
     }
-    __syncthreads();
-    if (warp == 0) {
-        const unsigned v = lane < E ? pre[lane] : 0u;
-        unsigned inc = v;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const unsigned t = __shfl_up_sync(0xffffffffu, inc, o);
-            if (lane >= o) inc += t;
-        }
-        if (lane < E) pre[lane] = inc - v;
-    }
-    __syncthreads();
+    scan_round_warp_counts<E>(pre);
     const unsigned run = ctx.blk_count[blockIdx.x];     // segments started before this block
 #pragma unroll
     for (int r = 0; r < SEGK_ITEMS; ++r) {

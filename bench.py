@@ -252,12 +252,13 @@ def kernel_bytes_per_particle(kind, w):
 
 # DRAM bytes (read + write) per particle per launch of the heaviest kernels, from
 # `ncu` captures of a 2,092,825-particle batch of the config-4 generator (FP32,
-# chained steps; profiles/reverse_particle_dram_config4_128scenes.md); their
-# traffic grows in proportion to the particles, so it is scaled to the workload.
+# chained steps; profiles/reverse_particle_dram_config4_128scenes.md and
+# profiles/g2p_per_model_config4_128scenes.md); their traffic grows in
+# proportion to the particles, so it is scaled to the workload.
 MEASURED_TRAFFIC_PER_PARTICLE = {
-    # the neo-Hookean and the Hencky run of one reverse step (the kernel specialised per model)
+    # the neo-Hookean and the Hencky run of one step (the kernels specialised per model)
     "bwd_particle": (281440768 + 89405440 + 244199680 + 81494016) / 2092825,
-    "g2p": (137.490688e6 + 339.093504e6) / 2092825,
+    "g2p": (73642240 + 131875328 + 63985408 + 110647808) / 2092825,
 }
 
 

@@ -268,7 +268,7 @@ int run_radix(MpmPlan* P, const unsigned* kin, const unsigned* vin, unsigned* ko
     const int tile = SORT_THREADS * ITEMS;
     const unsigned* ksrc = kin;
     const unsigned* vsrc = vin;
-    // the movers' sort (a device-side count, typically a few hundred of the nblk
+    // the movers' sort (a device-side count, typically about a hundred of the nblk
     // possible 256-key tiles): 4 blocks per SM stride over the active tiles
     // instead of one block per possible tile
     const int grid = ITEMS == 1 ? std::max(1, std::min(nblk, P->n_sm * 4)) : nblk;

@@ -197,7 +197,7 @@ constexpr int SEG_THREADS = 256;
 // block base + round*256 + thread, every key load coalesced), all their loads
 // issued before any is used, few registers: a block waits on one chain of
 // memory latencies (key, then its scene), not one per round.
-#ifndef MPM_SEGK_ITEMS
+#ifndef MPM_SEGK_ITEMS          // slots per thread (build-time; 4 measured fastest of 1, 2, 4, 8)
 #define MPM_SEGK_ITEMS 4
 #endif
 constexpr int SEGK_ITEMS = MPM_SEGK_ITEMS;
@@ -314,11 +314,8 @@ scan_counts_kernel(unsigned* __restrict__ cnt, int nblk, int* __restrict__ total
 __global__ void __launch_bounds__(256)
 remark_cells_kernel(Ctx ctx, const unsigned* __restrict__ skeys) {
     const int nseg = *ctx.n_seg;
-#ifndef MPM_REMARK_BATCH
-#define MPM_REMARK_BATCH 4
-#endif
-    // MPM_REMARK_BATCH segments per thread and pass, their loads issued together
-    constexpr int NB = MPM_REMARK_BATCH;
+    // NB segments per thread and pass, their loads issued together
+    constexpr int NB = 4;
     const int stride = gridDim.x * blockDim.x;
     for (int id0 = blockIdx.x * blockDim.x + threadIdx.x; id0 < nseg; id0 += NB * stride) {
         int f[NB];
@@ -372,7 +369,7 @@ __device__ __forceinline__ void scan_round_warp_counts(unsigned* pre) {
 // next step.  A block covers TILEK_ITEMS warp-striped rounds of tiles (every
 // load coalesced), and all its flag loads are issued before any is used; one
 // scan of the (round, warp) counts replaces a barrier pair per round.
-#ifndef MPM_TILEK_ITEMS
+#ifndef MPM_TILEK_ITEMS         // tiles per thread (build-time; 4 measured faster than 16)
 #define MPM_TILEK_ITEMS 4
 #endif
 constexpr int TILEK_ITEMS = MPM_TILEK_ITEMS;
